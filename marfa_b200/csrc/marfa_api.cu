@@ -1,0 +1,796 @@
+// marfa_api.cu -- host side of libmarfa_gpu.so: the C ABI of include/marfa_gpu.h.
+//
+// The host work per call is the part of the reference's driver that is cheap
+// and sequential: the subinterval loop bounds (main.f90:117-122, 171-172), the
+// starting line (main.f90:196-248) and the per-subinterval line window
+// recurrence of lblScheme (LBL.f90:41-61 with capWV of main.f90:138-144).
+// Everything per line and per grid point runs on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "marfa_gpu.h"
+#include "marfa_kernels.cuh"
+
+using namespace marfa;
+
+namespace {
+
+constexpr int64_t FAR_CHUNK = 4096; // lines per far-kernel block
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+} // namespace
+
+struct marfa_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t n_lines = 0;
+  std::vector<double> nu;  // host copy of the sorted centres (window scan)
+  double smax = 0.0;       // largest reference intensity
+  double dmin = 0.0, dmax = 0.0;
+  int n_iso = 0, n_temp = 0;
+  // line list, structure of arrays
+  double *d_nu = nullptr;
+  float *d_S = nullptr, *d_gair = nullptr, *d_gself = nullptr, *d_elow = nullptr,
+        *d_nair = nullptr, *d_delta = nullptr;
+  int *d_iso = nullptr;
+  double *d_tips = nullptr;
+  int *d_err = nullptr;
+  // grow-only work buffers
+  DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
+      b_out, b_out64, b_dump, b_count;
+  std::string err;
+  std::vector<cudaEvent_t> events;
+  // timing marks of the last compute call: (family, start, stop); family 5
+  // is the whole call
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  int launches = 0, far_launches = 0;
+};
+
+namespace {
+
+int set_err(marfa_ctx *c, int code, const char *fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+int cuda_fail(marfa_ctx *c, cudaError_t e, const char *where) {
+  if (e == cudaErrorMemoryAllocation)
+    return set_err(c, MARFA_E_NOMEM, "%s: %s", where, cudaGetErrorString(e));
+  return set_err(c, MARFA_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define CK(call, where)                                      \
+  do {                                                       \
+    cudaError_t e__ = (call);                                \
+    if (e__ != cudaSuccess) return cuda_fail(ctx, e__, where); \
+  } while (0)
+
+cudaError_t ensure(DevBuf &b, size_t bytes) {
+  if (bytes <= b.cap) return cudaSuccess;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  const size_t want = std::max(bytes, (size_t)256);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e == cudaSuccess) b.cap = want;
+  return e;
+}
+
+void release(DevBuf &b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+// Constants of Constants.f90 evaluated in double.
+Consts make_consts() {
+  Consts c;
+  c.pi = 3.1415926;
+  c.sqln2 = std::sqrt(std::log(2.0));
+  c.c2 = 6.626070e-27 * 2.99792458e10 / 1.3806503e-16;
+  c.doppler = std::sqrt(2.0 * 6.02214076e23 * 1.3806503e-16 * std::log(2.0)) / 2.99792458e10;
+  c.tref = 296.0;
+  c.bolsi = 1.3806503e-23;
+  c.stdp = 101325.0;
+  c.sqrtpi = std::sqrt(c.pi);
+  c.sqrt14 = std::sqrt(1.4);
+  return c;
+}
+
+// Subinterval bounds, windows and far-kernel chunks of one run.
+struct Plan {
+  int n_sub = 0;
+  std::vector<double> s, e;       // start / end of each subinterval
+  std::vector<int64_t> lo, hi;    // line window [lo, hi), 0-based
+  std::vector<int> chunk_sub;
+  std::vector<int64_t> chunk_begin, chunk_end;
+  std::vector<int> sub_chunk0;    // n_sub + 1
+};
+
+// Windows of all subintervals; returns 0 or MARFA_E_DB with `bad` = the
+// subinterval whose scan ran off the end (-1: before the starting line).
+int plan_windows(const double *nu, int64_t n, double start_wv, double end_wv, double cut,
+                 std::vector<double> &ss, std::vector<double> &se, std::vector<int64_t> &lo,
+                 std::vector<int64_t> &hi, int &bad) {
+  const int nsub = marfa_num_subintervals(start_wv, end_wv);
+  bad = -1;
+  // determineStartingSpectralLine (main.f90:196-248)
+  int64_t start_idx = 0;
+  double start_line = nu[0];
+  if (start_wv > cut) {
+    const double ext = start_wv - cut;
+    int64_t i = 0;
+    while (nu[i] <= ext)
+      if (++i >= n) return MARFA_E_DB;
+    start_idx = i;
+    start_line = nu[i];
+  }
+  // SUBINTERVALS_LOOP with the lblScheme window recurrence
+  int64_t line_idx = start_idx;
+  double s = start_wv;
+  for (int isub = 0; isub < nsub; ++isub) {
+    const double ext_end = s + DELTA_WV + cut;
+    double cap = (s - cut) + DELTA_WV;
+    if (cap <= start_line) cap = start_line;
+    int64_t I = line_idx, next = line_idx;
+    for (;; ++I) {
+      if (I >= n) {
+        bad = isub;
+        return MARFA_E_DB;
+      }
+      const double v = nu[I];
+      if (v >= ext_end) break;
+      if (v <= cap) next = I;
+    }
+    ss.push_back(s);
+    se.push_back(s + DELTA_WV);
+    lo.push_back(line_idx);
+    hi.push_back(I);
+    line_idx = next;
+    s = s + DELTA_WV;
+  }
+  return MARFA_OK;
+}
+
+int make_plan(marfa_ctx *ctx, const marfa_run *run, Plan &pl) {
+  pl.n_sub = marfa_num_subintervals(run->start_wv, run->end_wv);
+  int bad = -1;
+  if (plan_windows(ctx->nu.data(), ctx->n_lines, run->start_wv, run->end_wv, run->cutoff, pl.s, pl.e,
+                   pl.lo, pl.hi, bad))
+    return set_err(ctx, MARFA_E_DB,
+                   bad < 0 ? "line list ends before start - cutoff"
+                           : "line list ends inside a subinterval window (add a sentinel line beyond "
+                             "end + 10 + cutoff)");
+  pl.sub_chunk0.assign(pl.n_sub + 1, 0);
+  for (int isub = 0; isub < pl.n_sub; ++isub) {
+    pl.sub_chunk0[isub] = (int)pl.chunk_sub.size();
+    for (int64_t b = pl.lo[isub]; b < pl.hi[isub]; b += FAR_CHUNK) {
+      pl.chunk_sub.push_back(isub);
+      pl.chunk_begin.push_back(b);
+      pl.chunk_end.push_back(std::min(b + FAR_CHUNK, pl.hi[isub]));
+    }
+  }
+  pl.sub_chunk0[pl.n_sub] = (int)pl.chunk_sub.size();
+  return MARFA_OK;
+}
+
+int check_run(marfa_ctx *ctx, const marfa_run *run) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!run) return set_err(ctx, MARFA_E_ARG, "run is null");
+  if (!(run->cutoff > 0.0) || !std::isfinite(run->cutoff) || run->cutoff > 4000.0)
+    return set_err(ctx, MARFA_E_ARG, "cutoff must be in (0, 4000] cm-1");
+  if (!std::isfinite(run->start_wv) || !std::isfinite(run->end_wv))
+    return set_err(ctx, MARFA_E_ARG, "non-finite spectral interval");
+  if (run->target != MARFA_TARGET_ACS && run->target != MARFA_TARGET_VAC)
+    return set_err(ctx, 2, "target must be ACS or VAC");
+  if (run->chi < MARFA_CHI_NONE || run->chi > MARFA_CHI_PERRIN)
+    return set_err(ctx, MARFA_E_ARG, "unknown chi-factor %d", run->chi);
+  if (run->shape != MARFA_SHAPE_VOIGT && run->shape != MARFA_SHAPE_ONE && run->shape != MARFA_SHAPE_ABSX)
+    return set_err(ctx, MARFA_E_ARG, "unknown shape %d", run->shape);
+  if (run->precision != MARFA_PREC_FP64 && run->precision != MARFA_PREC_FP32C)
+    return set_err(ctx, MARFA_E_ARG, "unknown precision %d", run->precision);
+  if (run->mol_code < 1 || run->mol_code > 12) return set_err(ctx, 8, "unsupported molecule code %d", run->mol_code);
+  return MARFA_OK;
+}
+
+int build_levels(marfa_ctx *ctx, int n, const double *P, const double *T, const double *dens,
+                 std::vector<LevelConst> &lv) {
+  const Consts c = make_consts();
+  lv.resize(n);
+  for (int l = 0; l < n; ++l) {
+    if (!std::isfinite(P[l]) || !std::isfinite(T[l]) || !std::isfinite(dens[l]) || P[l] < 0.0)
+      return set_err(ctx, 7, "level %d: invalid pressure/temperature/density", l + 1);
+    const double tval = (T[l] - 20.0) / 2.0 + 1.0;
+    const int idx = (int)tval;
+    if (!(tval >= 1.0) || idx + 1 > ctx->n_temp)
+      return set_err(ctx, MARFA_E_TEMPERATURE, "level %d: temperature %.3f K outside the TIPS table",
+                     l + 1, T[l]);
+    LevelConst &v = lv[l];
+    v.P = P[l];
+    v.T = T[l];
+    v.density = dens[l];
+    v.pself = dens[l] * 10.0 * c.bolsi * T[l] / c.stdp; // main.f90:92
+    v.perrin_b1 = 0.0888 - 0.16 * std::exp(-(0.00410 * T[l]));
+    v.perrin_b2 = 0.0526 * std::exp(-(0.00152 * T[l]));
+  }
+  return MARFA_OK;
+}
+
+struct Outputs {
+  float *host_out = nullptr;     // host records (copied per level chunk)
+  double *host_out64 = nullptr;
+  float *dev_out = nullptr;      // device records (written in place)
+  double *host_dump = nullptr;   // raw accumulators of one unit
+  int dump_level = -1, dump_sub = -1;
+};
+
+// The whole computation for a flat list of levels.
+int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *P,
+               const double *T, const double *dens, const Outputs &o, cudaStream_t st) {
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  if (n_levels < 1 || !P || !T || !dens) return set_err(ctx, MARFA_E_ARG, "no levels");
+  Plan pl;
+  if ((rc = make_plan(ctx, run, pl))) return rc;
+  std::vector<LevelConst> lv;
+  if ((rc = build_levels(ctx, n_levels, P, T, dens, lv))) return rc;
+  const int nsub = pl.n_sub;
+  if (nsub == 0) return MARFA_OK;
+  const int64_t N = ctx->n_lines;
+  const bool f64 = run->precision == MARFA_PREC_FP64;
+  const int chi = run->mol_code == 2 ? run->chi : MARFA_CHI_NONE; // CO2-only factors
+  const int C = (int)pl.chunk_sub.size();
+  const Consts cst = make_consts();
+
+  // FP32-compensated form: scale intensities by 2^E so that every partial
+  // sum stays far from the float underflow and overflow limits.
+  double sscale = 1.0;
+  if (!f64) {
+    const double top = std::max(ctx->smax, 1e-300) * 3e7;
+    int E = 60 - (int)std::ceil(std::log2(top));
+    E = std::max(-100, std::min(120, E));
+    sscale = std::ldexp(1.0, E);
+  }
+
+  // memory plan: levels per chunk and units per fine/cascade batch
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  const size_t per_level = (size_t)N * (8 + sizeof(LineGen) + (f64 ? sizeof(Hot64) : sizeof(Hot32)) + 8 + 8 + 4) +
+                           (size_t)C * NFAR * 8 + (size_t)nsub * NT * (o.dev_out ? 0 : 4) +
+                           (o.host_out64 ? (size_t)nsub * NT * 8 : 0);
+  const size_t reuse = ctx->b_nus.cap + ctx->b_gen.cap + ctx->b_hot.cap + ctx->b_rank.cap + ctx->b_snu.cap +
+                       ctx->b_sidx.cap + ctx->b_far.cap + ctx->b_out.cap + ctx->b_out64.cap;
+  const size_t budget = (size_t)((double)(free_b + reuse) * 0.55);
+  int Lc = (int)std::max<size_t>(1, std::min<size_t>((size_t)n_levels, budget / std::max<size_t>(per_level, 1)));
+  const size_t elem = f64 ? 8 : 4;
+  const size_t unit_bytes = (size_t)SCR_STRIDE * elem;
+  const size_t scr_budget = std::max<size_t>(unit_bytes, std::min<size_t>((size_t)4 << 30, (free_b + ctx->b_scr.cap) / 5));
+  int UB = (int)std::max<size_t>(1, std::min<size_t>((size_t)Lc * nsub, scr_budget / unit_bytes));
+
+  CK(ensure(ctx->b_nus, (size_t)Lc * N * 8), "alloc nus");
+  CK(ensure(ctx->b_gen, (size_t)Lc * N * sizeof(LineGen)), "alloc gen");
+  CK(ensure(ctx->b_hot, (size_t)Lc * N * (f64 ? sizeof(Hot64) : sizeof(Hot32))), "alloc hot");
+  CK(ensure(ctx->b_rank, (size_t)Lc * N * 8), "alloc rank");
+  CK(ensure(ctx->b_snu, (size_t)Lc * N * 8), "alloc snu");
+  CK(ensure(ctx->b_sidx, (size_t)Lc * N * 4), "alloc sidx");
+  CK(ensure(ctx->b_far, (size_t)Lc * std::max(C, 1) * NFAR * 8), "alloc far");
+  CK(ensure(ctx->b_scr, (size_t)UB * unit_bytes), "alloc scratch");
+  CK(ensure(ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
+  CK(ensure(ctx->b_margin, (size_t)n_levels * 8), "alloc margin");
+  if (!o.dev_out) CK(ensure(ctx->b_out, (size_t)Lc * nsub * NT * 4), "alloc out");
+  if (o.host_out64) CK(ensure(ctx->b_out64, (size_t)Lc * nsub * NT * 8), "alloc out64");
+  if (o.host_dump) CK(ensure(ctx->b_dump, (size_t)(NT + 3 * NCELLS) * 8), "alloc dump");
+  // window and chunk tables
+  const size_t win_bytes = (size_t)nsub * (8 + 8 + 8 + 8) + (size_t)(nsub + 1) * 4;
+  CK(ensure(ctx->b_win, win_bytes), "alloc windows");
+  const size_t chunk_bytes = (size_t)std::max(C, 1) * (4 + 8 + 8);
+  CK(ensure(ctx->b_chunks, chunk_bytes), "alloc chunks");
+
+  char *wb = (char *)ctx->b_win.p;
+  double *d_s = (double *)wb;
+  double *d_e = d_s + nsub;
+  int64_t *d_lo = (int64_t *)(d_e + nsub);
+  int64_t *d_hi = d_lo + nsub;
+  int *d_sc0 = (int *)(d_hi + nsub);
+  char *cb = (char *)ctx->b_chunks.p;
+  int64_t *d_cb = (int64_t *)cb;
+  int64_t *d_ce = d_cb + std::max(C, 1);
+  int *d_cs = (int *)(d_ce + std::max(C, 1));
+  CK(cudaMemcpyAsync(d_s, pl.s.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
+  CK(cudaMemcpyAsync(d_e, pl.e.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
+  CK(cudaMemcpyAsync(d_lo, pl.lo.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
+  CK(cudaMemcpyAsync(d_hi, pl.hi.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
+  CK(cudaMemcpyAsync(d_sc0, pl.sub_chunk0.data(), (nsub + 1) * 4, cudaMemcpyHostToDevice, st), "h2d windows");
+  if (C > 0) {
+    CK(cudaMemcpyAsync(d_cb, pl.chunk_begin.data(), C * 8, cudaMemcpyHostToDevice, st), "h2d chunks");
+    CK(cudaMemcpyAsync(d_ce, pl.chunk_end.data(), C * 8, cudaMemcpyHostToDevice, st), "h2d chunks");
+    CK(cudaMemcpyAsync(d_cs, pl.chunk_sub.data(), C * 4, cudaMemcpyHostToDevice, st), "h2d chunks");
+  }
+  std::vector<double> margin(n_levels);
+  for (int l = 0; l < n_levels; ++l) {
+    const double a = ctx->dmin * P[l], b = ctx->dmax * P[l];
+    margin[l] = std::fabs(b - a) + 1e-7 + 1e-12 * std::fabs(ctx->nu.back());
+  }
+  LevelConst *d_lv = (LevelConst *)ctx->b_lv.p;
+  double *d_margin = (double *)ctx->b_margin.p;
+  CK(cudaMemcpyAsync(d_lv, lv.data(), n_levels * sizeof(LevelConst), cudaMemcpyHostToDevice, st), "h2d levels");
+  CK(cudaMemcpyAsync(d_margin, margin.data(), n_levels * 8, cudaMemcpyHostToDevice, st), "h2d margin");
+  CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st), "memset err");
+
+  WindowTable win{d_s, d_e, d_lo, d_hi, nsub};
+  DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N};
+
+  // timing events of every kernel family, resolved by marfa_last_timings
+  ctx->marks.clear();
+  ctx->launches = 0;
+  ctx->far_launches = 0;
+  auto mark = [&](int fam, cudaEvent_t a, cudaEvent_t b) { ctx->marks.push_back({fam, {a, b}}); };
+  size_t ev_used = 0;
+  auto next_event = [&]() -> cudaEvent_t {
+    if (ev_used == ctx->events.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      ctx->events.push_back(e);
+    }
+    return ctx->events[ev_used++];
+  };
+  cudaEvent_t ev_begin = next_event();
+  if (ev_begin) cudaEventRecord(ev_begin, st);
+
+  for (int l0 = 0; l0 < n_levels; l0 += Lc) {
+    const int nl = std::min(Lc, n_levels - l0);
+    PrepParams pp;
+    pp.lines = dl;
+    pp.tips = ctx->d_tips;
+    pp.n_iso = ctx->n_iso;
+    pp.n_temp = ctx->n_temp;
+    pp.lv = d_lv + l0;
+    pp.n_levels = nl;
+    pp.c = cst;
+    pp.sscale = sscale;
+    pp.nus = (double *)ctx->b_nus.p;
+    pp.gen = (LineGen *)ctx->b_gen.p;
+    pp.hot32 = f64 ? nullptr : (Hot32 *)ctx->b_hot.p;
+    pp.hot64 = f64 ? (Hot64 *)ctx->b_hot.p : nullptr;
+    pp.err = ctx->d_err;
+    cudaEvent_t e0 = next_event(), e1 = next_event(), e2 = next_event(), e3 = next_event();
+    if (e0) cudaEventRecord(e0, st);
+    CK(launch_prep(pp, st), "prep kernel");
+    ctx->launches += 1;
+    if (e1) cudaEventRecord(e1, st);
+    SortParams sp;
+    sp.nu = ctx->d_nu;
+    sp.nus = pp.nus;
+    sp.margin = d_margin + l0;
+    sp.n = N;
+    sp.n_levels = nl;
+    sp.rank = (int64_t *)ctx->b_rank.p;
+    sp.snu = (double *)ctx->b_snu.p;
+    sp.sidx = (int *)ctx->b_sidx.p;
+    CK(launch_sort(sp, st), "sort kernels");
+    ctx->launches += 2;
+    if (e2) cudaEventRecord(e2, st);
+    FarParams fp;
+    fp.nus = pp.nus;
+    fp.hot32 = pp.hot32;
+    fp.hot64 = pp.hot64;
+    fp.gen = pp.gen;
+    fp.lv = pp.lv;
+    fp.win = win;
+    fp.chunk_sub = d_cs;
+    fp.chunk_begin = d_cb;
+    fp.chunk_end = d_ce;
+    fp.n_chunks = C;
+    fp.n_levels = nl;
+    fp.n_lines = N;
+    fp.cutoff = run->cutoff;
+    fp.sscale = sscale;
+    fp.shape = run->shape;
+    fp.c = cst;
+    fp.out = (double *)ctx->b_far.p;
+    CK(launch_far(fp, run->precision, chi, st), "far kernel");
+    if (C > 0) {
+      ctx->launches += 1;
+      ctx->far_launches += 1;
+    }
+    if (e3) cudaEventRecord(e3, st);
+    mark(0, e0, e1);
+    mark(1, e1, e2);
+    mark(2, e2, e3);
+
+    float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p;
+    const int out_level0 = o.dev_out ? l0 : 0;
+    const int units = nl * nsub;
+    for (int u0 = 0; u0 < units; u0 += UB) {
+      const int nu_ = std::min(UB, units - u0);
+      FineParams fn;
+      fn.snu = sp.snu;
+      fn.sidx = sp.sidx;
+      fn.gen = pp.gen;
+      fn.lv = pp.lv;
+      fn.win = win;
+      fn.n_lines = N;
+      fn.unit0 = u0;
+      fn.n_units = nu_;
+      fn.cutoff = run->cutoff;
+      fn.sscale = sscale;
+      fn.shape = run->shape;
+      fn.c = cst;
+      fn.scratch = ctx->b_scr.p;
+      cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
+      if (f0) cudaEventRecord(f0, st);
+      CK(launch_fine(fn, run->precision, chi, st), "fine kernel");
+      ctx->launches += 1;
+      if (f1) cudaEventRecord(f1, st);
+      CascadeParams cp;
+      cp.scratch = ctx->b_scr.p;
+      cp.far = fp.out;
+      cp.sub_chunk0 = d_sc0;
+      cp.lv = pp.lv;
+      cp.n_chunks = C;
+      cp.n_sub = nsub;
+      cp.unit0 = u0;
+      cp.n_units = nu_;
+      cp.level_out0 = out_level0;
+      cp.inv_sscale = 1.0 / sscale;
+      cp.target = run->target;
+      cp.out = out_base;
+      cp.out64 = o.host_out64 ? (double *)ctx->b_out64.p : nullptr;
+      cp.dump = nullptr;
+      cp.dump_unit = -1;
+      if (o.host_dump && o.dump_level >= l0 && o.dump_level < l0 + nl) {
+        cp.dump = (double *)ctx->b_dump.p;
+        cp.dump_unit = (o.dump_level - l0) * nsub + o.dump_sub;
+      }
+      CK(launch_cascade(cp, run->precision, st), "cascade kernel");
+      ctx->launches += cp.dump ? 2 : 1;
+      if (f2) cudaEventRecord(f2, st);
+      mark(3, f0, f1);
+      mark(4, f1, f2);
+    }
+    if (o.host_out)
+      CK(cudaMemcpyAsync(o.host_out + (size_t)l0 * nsub * NT, ctx->b_out.p, (size_t)nl * nsub * NT * 4,
+                         cudaMemcpyDeviceToHost, st), "d2h records");
+    if (o.host_out64)
+      CK(cudaMemcpyAsync(o.host_out64 + (size_t)l0 * nsub * NT, ctx->b_out64.p, (size_t)nl * nsub * NT * 8,
+                         cudaMemcpyDeviceToHost, st), "d2h records64");
+  }
+  cudaEvent_t ev_end = next_event();
+  if (ev_end) cudaEventRecord(ev_end, st);
+  if (ev_begin && ev_end) mark(5, ev_begin, ev_end);
+  if (o.host_dump)
+    CK(cudaMemcpyAsync(o.host_dump, ctx->b_dump.p, (size_t)(NT + 3 * NCELLS) * 8, cudaMemcpyDeviceToHost, st),
+       "d2h dump");
+  if (o.dev_out) return MARFA_OK; // asynchronous path: caller synchronises
+  CK(cudaStreamSynchronize(st), "stream sync");
+  int herr = 0;
+  CK(cudaMemcpy(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost), "d2h err");
+  if (herr) return set_err(ctx, herr, "device reported status %d (isotopologue or temperature outside tables)", herr);
+  return MARFA_OK;
+}
+
+int total_levels(marfa_ctx *ctx, int n_profiles, const int *counts, int &total) {
+  total = 0;
+  if (n_profiles < 1 || !counts) return set_err(ctx, MARFA_E_ARG, "no profiles");
+  for (int i = 0; i < n_profiles; ++i) {
+    if (counts[i] < 1) return set_err(ctx, MARFA_E_ARG, "profile %d has no levels", i);
+    if (counts[i] > 200) return set_err(ctx, 6, "profile %d has %d levels > 200", i, counts[i]);
+    total += counts[i];
+  }
+  return MARFA_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int marfa_num_subintervals(double start_wv, double end_wv) {
+  int n = 0;
+  double s = start_wv;
+  while (s < end_wv) {
+    ++n;
+    s = s + DELTA_WV;
+  }
+  return n;
+}
+
+int marfa_record_number(double start_wv, int isub) {
+  double s = start_wv;
+  for (int i = 0; i < isub; ++i) s = s + DELTA_WV;
+  return (int)((s + 1.0) / 10.0);
+}
+
+int marfa_plan_windows(const double *nu, int64_t n_lines, double start_wv, double end_wv, double cutoff,
+                       int64_t *lo, int64_t *hi) {
+  if (!nu || n_lines < 1 || !lo || !hi) return MARFA_E_ARG;
+  try {
+    std::vector<double> ss, se;
+    std::vector<int64_t> l, h;
+    int bad = -1;
+    const int rc = plan_windows(nu, n_lines, start_wv, end_wv, cutoff, ss, se, l, h, bad);
+    if (rc) return rc;
+    for (size_t i = 0; i < l.size(); ++i) {
+      lo[i] = l[i];
+      hi[i] = h[i];
+    }
+    return MARFA_OK;
+  } catch (...) {
+    return MARFA_E_NOMEM;
+  }
+}
+
+int marfa_ctx_create(const marfa_line_record *lines, int64_t n_lines, const double *tips, int n_iso,
+                     int n_temp, int device, marfa_ctx **out) {
+  if (!out) return MARFA_E_ARG;
+  *out = nullptr;
+  if (!lines || n_lines < 1 || !tips || n_iso < 1 || n_temp < 139 || n_lines > 2000000000LL)
+    return MARFA_E_ARG;
+  marfa_ctx *ctx = new (std::nothrow) marfa_ctx();
+  if (!ctx) return MARFA_E_NOMEM;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    delete ctx;
+    return MARFA_E_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    delete ctx;
+    return MARFA_E_ARG;
+  }
+  ctx->device = device;
+  ctx->n_lines = n_lines;
+  ctx->n_iso = n_iso;
+  ctx->n_temp = n_temp;
+  ctx->nu.resize(n_lines);
+  std::vector<float> S(n_lines), ga(n_lines), gs(n_lines), el(n_lines), na(n_lines), de(n_lines);
+  std::vector<int> iso(n_lines);
+  ctx->dmin = 1e300;
+  ctx->dmax = -1e300;
+  for (int64_t i = 0; i < n_lines; ++i) {
+    const marfa_line_record &r = lines[i];
+    if (!std::isfinite(r.nu) || (i > 0 && r.nu < lines[i - 1].nu)) {
+      delete ctx;
+      return MARFA_E_UNSORTED;
+    }
+    ctx->nu[i] = r.nu;
+    S[i] = r.S;
+    ga[i] = r.gamma_air;
+    gs[i] = r.gamma_self;
+    el[i] = r.e_lower;
+    na[i] = r.n_air;
+    de[i] = r.delta_air;
+    iso[i] = r.joint_mol_iso / 100;
+    ctx->smax = std::max(ctx->smax, (double)std::fabs(r.S));
+    ctx->dmin = std::min(ctx->dmin, (double)r.delta_air);
+    ctx->dmax = std::max(ctx->dmax, (double)r.delta_air);
+  }
+  int rc = MARFA_OK;
+  auto fail = [&](cudaError_t e, const char *w) {
+    rc = cuda_fail(ctx, e, w);
+    return rc;
+  };
+  cudaError_t e;
+  if ((e = cudaSetDevice(device)) != cudaSuccess) fail(e, "cudaSetDevice");
+  if (!rc && (e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    fail(e, "stream");
+  const size_t nb8 = (size_t)n_lines * 8, nb4 = (size_t)n_lines * 4;
+  void **ptrs[] = {(void **)&ctx->d_nu, (void **)&ctx->d_S, (void **)&ctx->d_gair, (void **)&ctx->d_gself,
+                   (void **)&ctx->d_elow, (void **)&ctx->d_nair, (void **)&ctx->d_delta, (void **)&ctx->d_iso};
+  const void *src[] = {ctx->nu.data(), S.data(), ga.data(), gs.data(), el.data(), na.data(), de.data(), iso.data()};
+  for (int k = 0; k < 8 && !rc; ++k) {
+    const size_t nb = k == 0 ? nb8 : nb4;
+    if ((e = cudaMalloc(ptrs[k], nb)) != cudaSuccess) fail(e, "alloc lines");
+    else if ((e = cudaMemcpy(*ptrs[k], src[k], nb, cudaMemcpyHostToDevice)) != cudaSuccess) fail(e, "h2d lines");
+  }
+  if (!rc && (e = cudaMalloc(&ctx->d_tips, (size_t)n_iso * n_temp * 8)) != cudaSuccess) fail(e, "alloc tips");
+  if (!rc && (e = cudaMemcpy(ctx->d_tips, tips, (size_t)n_iso * n_temp * 8, cudaMemcpyHostToDevice)) != cudaSuccess)
+    fail(e, "h2d tips");
+  if (!rc && (e = cudaMalloc(&ctx->d_err, sizeof(int))) != cudaSuccess) fail(e, "alloc err");
+  if (rc) {
+    int code = rc;
+    marfa_ctx_destroy(ctx);
+    return code;
+  }
+  *out = ctx;
+  return MARFA_OK;
+}
+
+void marfa_ctx_destroy(marfa_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  void *ps[] = {ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta,
+                ctx->d_iso, ctx->d_tips, ctx->d_err};
+  for (void *p : ps)
+    if (p) cudaFree(p);
+  DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
+                  &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
+                  &ctx->b_out64, &ctx->b_dump, &ctx->b_count};
+  for (DevBuf *b : bs) release(*b);
+  for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char *marfa_last_error(const marfa_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int marfa_compute_batched(marfa_ctx *ctx, const marfa_run *run, int n_profiles, const int *level_counts,
+                          const double *pressure, const double *temperature, const double *density,
+                          float *out, double *out64) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!out) return set_err(ctx, MARFA_E_ARG, "out is null");
+  int total = 0, rc = total_levels(ctx, n_profiles, level_counts, total);
+  if (rc) return rc;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+  Outputs o;
+  o.host_out = out;
+  o.host_out64 = out64;
+  try {
+    return run_levels(ctx, run, total, pressure, temperature, density, o, ctx->stream);
+  } catch (...) {
+    return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
+  }
+}
+
+int marfa_compute(marfa_ctx *ctx, const marfa_run *run, const double *pressure, const double *temperature,
+                  const double *density, int n_levels, float *out, double *out64) {
+  return marfa_compute_batched(ctx, run, 1, &n_levels, pressure, temperature, density, out, out64);
+}
+
+int marfa_compute_device(marfa_ctx *ctx, const marfa_run *run, int n_profiles, const int *level_counts,
+                         const double *pressure, const double *temperature, const double *density,
+                         float *device_out, void *stream) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!device_out) return set_err(ctx, MARFA_E_ARG, "device_out is null");
+  int total = 0, rc = total_levels(ctx, n_profiles, level_counts, total);
+  if (rc) return rc;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+  Outputs o;
+  o.dev_out = device_out;
+  try {
+    return run_levels(ctx, run, total, pressure, temperature, density, o,
+                      stream ? (cudaStream_t)stream : ctx->stream);
+  } catch (...) {
+    return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
+  }
+}
+
+int marfa_synchronize(marfa_ctx *ctx) {
+  if (!ctx) return MARFA_E_ARG;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "synchronize");
+  int herr = 0;
+  e = cudaMemcpy(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "d2h err");
+  if (herr) return set_err(ctx, herr, "device reported status %d", herr);
+  return MARFA_OK;
+}
+
+int marfa_eval_count(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *pressure,
+                     const double *temperature, const double *density, int64_t *evals, int64_t *far_evals) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!evals) return set_err(ctx, MARFA_E_ARG, "evals is null");
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  try {
+    Plan pl;
+    if ((rc = make_plan(ctx, run, pl))) return rc;
+    std::vector<LevelConst> lv;
+    if ((rc = build_levels(ctx, n_levels, pressure, temperature, density, lv))) return rc;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    const int64_t N = ctx->n_lines;
+    const int nsub = pl.n_sub, C = (int)pl.chunk_sub.size();
+    for (int l = 0; l < n_levels; ++l) {
+      evals[l] = 0;
+      if (far_evals) far_evals[l] = 0;
+    }
+    if (C == 0) return MARFA_OK;
+    CK(ensure(ctx->b_nus, (size_t)N * 8), "alloc nus");
+    CK(ensure(ctx->b_gen, (size_t)N * sizeof(LineGen)), "alloc gen");
+    CK(ensure(ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
+    CK(ensure(ctx->b_win, (size_t)nsub * 32), "alloc windows");
+    CK(ensure(ctx->b_chunks, (size_t)C * 20), "alloc chunks");
+    CK(ensure(ctx->b_count, (size_t)C * 16), "alloc count");
+    double *d_s = (double *)ctx->b_win.p, *d_e = d_s + nsub;
+    int64_t *d_cb = (int64_t *)ctx->b_chunks.p, *d_ce = d_cb + C;
+    int *d_cs = (int *)(d_ce + C);
+    CK(cudaMemcpyAsync(d_s, pl.s.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d");
+    CK(cudaMemcpyAsync(d_e, pl.e.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d");
+    CK(cudaMemcpyAsync(d_cb, pl.chunk_begin.data(), C * 8, cudaMemcpyHostToDevice, st), "h2d");
+    CK(cudaMemcpyAsync(d_ce, pl.chunk_end.data(), C * 8, cudaMemcpyHostToDevice, st), "h2d");
+    CK(cudaMemcpyAsync(d_cs, pl.chunk_sub.data(), C * 4, cudaMemcpyHostToDevice, st), "h2d");
+    CK(cudaMemcpyAsync(ctx->b_lv.p, lv.data(), n_levels * sizeof(LevelConst), cudaMemcpyHostToDevice, st), "h2d");
+    CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st), "memset");
+    std::vector<unsigned long long> cnt(2 * (size_t)C);
+    DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N};
+    for (int l = 0; l < n_levels; ++l) {
+      PrepParams pp{};
+      pp.lines = dl;
+      pp.tips = ctx->d_tips;
+      pp.n_iso = ctx->n_iso;
+      pp.n_temp = ctx->n_temp;
+      pp.lv = (LevelConst *)ctx->b_lv.p + l;
+      pp.n_levels = 1;
+      pp.c = make_consts();
+      pp.sscale = 1.0;
+      pp.nus = (double *)ctx->b_nus.p;
+      pp.gen = (LineGen *)ctx->b_gen.p;
+      pp.err = ctx->d_err;
+      CK(launch_prep(pp, st), "prep kernel");
+      CountParams cp;
+      cp.nus = pp.nus;
+      cp.win = WindowTable{d_s, d_e, nullptr, nullptr, nsub};
+      cp.chunk_sub = d_cs;
+      cp.chunk_begin = d_cb;
+      cp.chunk_end = d_ce;
+      cp.n_chunks = C;
+      cp.n_levels = 1;
+      cp.n_lines = N;
+      cp.cutoff = run->cutoff;
+      cp.out = (unsigned long long *)ctx->b_count.p;
+      CK(launch_count(cp, st), "count kernel");
+      CK(cudaMemcpyAsync(cnt.data(), ctx->b_count.p, (size_t)C * 16, cudaMemcpyDeviceToHost, st), "d2h count");
+      CK(cudaStreamSynchronize(st), "sync");
+      for (int c = 0; c < C; ++c) {
+        evals[l] += (int64_t)cnt[2 * (size_t)c];
+        if (far_evals) far_evals[l] += (int64_t)cnt[2 * (size_t)c + 1];
+      }
+    }
+    return MARFA_OK;
+  } catch (...) {
+    return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
+  }
+}
+
+int marfa_debug_accumulators(marfa_ctx *ctx, const marfa_run *run, const double *pressure,
+                             const double *temperature, const double *density, int n_levels, int level,
+                             int isub, double *dump) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!dump || level < 0 || level >= n_levels || isub < 0 ||
+      (run && isub >= marfa_num_subintervals(run->start_wv, run->end_wv)))
+    return set_err(ctx, MARFA_E_ARG, "bad dump request");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+  try {
+    std::vector<float> tmp((size_t)n_levels * marfa_num_subintervals(run->start_wv, run->end_wv) * NT);
+    Outputs o;
+    o.host_out = tmp.data();
+    o.host_dump = dump;
+    o.dump_level = level;
+    o.dump_sub = isub;
+    return run_levels(ctx, run, n_levels, pressure, temperature, density, o, ctx->stream);
+  } catch (...) {
+    return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
+  }
+}
+
+int marfa_last_timings(marfa_ctx *ctx, double *times) {
+  if (!ctx || !times) return MARFA_E_ARG;
+  for (int i = 0; i < 8; ++i) times[i] = 0.0;
+  for (auto &m : ctx->marks) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(m.second.second) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "event sync");
+    if (cudaEventElapsedTime(&ms, m.second.first, m.second.second) == cudaSuccess) times[m.first] += ms;
+  }
+  times[6] = ctx->launches;
+  times[7] = ctx->far_launches;
+  return MARFA_OK;
+}
+
+} // extern "C"

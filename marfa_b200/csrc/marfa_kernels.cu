@@ -1,0 +1,1119 @@
+// marfa_kernels.cu -- the line-by-line kernels for sm_100a.
+//
+// Pipeline per chunk of atmospheric levels (one stream, no global atomics in
+// any accumulation):
+//   prep_kernel     per (level, line) spectroscopy in double: shifted centre,
+//                   Doppler / Lorentz HWHM, S(T) (Spectroscopy.f90:38-145,
+//                   LBL.f90:64-73).
+//   rank/scatter    per level, the lines ordered by shifted centre (the
+//                   pressure shift re-orders nearby lines) so that every
+//                   multigrid cell's contributing lines are one contiguous run.
+//   far_kernel      lines at least 1 cm-1 outside the subinterval: 21 grid-0
+//                   evaluations each, one thread per line, register sums,
+//                   block reduction (leftLBL / rightLBL grid-0 part).
+//   fine_kernel     lines within 1 cm-1 of / inside the subinterval: every
+//                   remaining accumulator (grid 0 near part, grids 1..9, direct
+//                   finest points) gathered per accumulator over its
+//                   contiguous run of lines (centerLBL and the fine-grid parts
+//                   of leftLBL / rightLBL).
+//   cascade_kernel  FP64 cascade interpolation per grid-0 cell subtree plus the
+//                   PT-record write (Grids.f90:80-139, main.f90:163-168).
+#include <cstdio>
+#include <type_traits>
+#include "marfa_kernels.cuh"
+#include "marfa_wiso.h"
+
+namespace marfa {
+
+__constant__ double c_wiso[MARFA_WISO_LEN];
+
+// ---------------------------------------------------------------- prep
+__global__ void __launch_bounds__(256) prep_kernel(PrepParams p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = blockIdx.y;
+  if (i >= p.lines.n) return;
+  const LevelConst lv = p.lv[l];
+  const Consts c = p.c;
+  const int iso = p.lines.iso[i];
+  const size_t o = (size_t)l * p.lines.n + i;
+  const double nu = p.lines.nu[i];
+  if (iso < 1 || iso > MARFA_WISO_LEN || iso > p.n_iso) {
+    atomicMax(p.err, 13);
+    p.nus[o] = nu;
+    return;
+  }
+  const double T = lv.T, P = lv.P;
+  const double M = c_wiso[iso - 1];
+  // shiftedLinePosition, dopplerHWHM, lorentzHWHM (Spectroscopy.f90:38-88)
+  const double nus = nu + (double)p.lines.delta[i] * P;
+  const double alpha = c.doppler * nus * sqrt(T / M);
+  const double gamma = pow(c.tref / T, (double)p.lines.nair[i]) *
+                       ((double)p.lines.gair[i] * (P - lv.pself) + (double)p.lines.gself[i] * lv.pself);
+  // TIPSofT (Spectroscopy.f90:91-115): linear interpolation in 2 K steps
+  const double tval = (T - 20.0) / 2.0 + 1.0;
+  const int idx = (int)tval;
+  double S = 0.0;
+  if (!(tval >= 1.0) || idx + 1 > p.n_temp) {
+    atomicMax(p.err, 11);
+  } else {
+    const double *row = p.tips + (size_t)(iso - 1) * p.n_temp;
+    const double lwt = (double)idx * 2.0 + 18.0;
+    const double uw = (T - lwt) / 2.0, lw = 1.0 - uw;
+    const double Q = lw * row[idx - 1] + uw * row[idx];
+    const double Qref = row[138];
+    if (!isfinite(Q) || !isfinite(Qref)) atomicMax(p.err, 13);
+    // intensityOfT (Spectroscopy.f90:118-145), unshifted nu in the emission term
+    const double E = (double)p.lines.elow[i];
+    const double boltz = exp(-(c.c2 * E / T)) / exp(-(c.c2 * E / c.tref));
+    const double emis = (1.0 - exp(-(c.c2 * nu / T))) / (1.0 - exp(-(c.c2 * nu / c.tref)));
+    S = (double)p.lines.S[i] * (Qref / Q) * boltz * emis;
+  }
+  LineGen g;
+  g.qx = c.sqln2 / alpha;
+  g.vy = c.sqln2 * gamma / alpha;
+  g.S = S;
+  g.alpha = alpha;
+  g.gamma = gamma;
+  g.lorA = gamma * S / c.pi;
+  p.nus[o] = nus;
+  p.gen[o] = g;
+  if (p.hot32) {
+    Hot32 h;
+    h.lorA = (float)(g.lorA * p.sscale);
+    h.g2 = (float)(gamma * gamma);
+    h.qx = g.qx;
+    p.hot32[o] = h;
+  }
+  if (p.hot64) {
+    Hot64 h;
+    h.lorA = g.lorA;
+    h.g2 = gamma * gamma;
+    h.qx = g.qx;
+    p.hot64[o] = h;
+  }
+}
+
+// ---------------------------------------------------------------- sort
+// Rank of line i among the shifted centres of its level (ties by index).  A
+// line can only change places with lines whose unshifted centre lies within
+// the level's shift spread, found by binary search on the sorted centres.
+__device__ __forceinline__ int64_t lower_bound_d(const double *a, int64_t n, double x) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t m = (lo + hi) >> 1;
+    if (a[m] < x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+__device__ __forceinline__ int64_t upper_bound_d(const double *a, int64_t n, double x) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t m = (lo + hi) >> 1;
+    if (a[m] <= x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) rank_kernel(SortParams p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = blockIdx.y;
+  if (i >= p.n) return;
+  const double *key = p.nus + (size_t)l * p.n;
+  const double m = p.margin[l];
+  const double nu = p.nu[i], k = key[i];
+  const int64_t jlo = lower_bound_d(p.nu, p.n, nu - m);
+  const int64_t jhi = upper_bound_d(p.nu, p.n, nu + m);
+  int64_t r = jlo;
+  for (int64_t j = jlo; j < jhi; ++j) {
+    const double kj = key[j];
+    r += (kj < k) || (kj == k && j < i);
+  }
+  p.rank[(size_t)l * p.n + i] = r;
+}
+
+__global__ void __launch_bounds__(256) scatter_kernel(SortParams p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = blockIdx.y;
+  if (i >= p.n) return;
+  const size_t o = (size_t)l * p.n;
+  const int64_t r = p.rank[o + i];
+  p.snu[o + r] = p.nus[o + i];
+  p.sidx[o + r] = (int)i;
+}
+
+// ------------------------------------------------------------ block reduce
+template <int N>
+__device__ __forceinline__ void block_reduce_store(double (&v)[N], double *dst) {
+  __shared__ double red[32][N];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double x = v[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if (lane == 0) red[warp][k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < N) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[w][threadIdx.x];
+    dst[threadIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------- far lines
+// Classification of one line against subinterval [s, se] (LBL.f90:81-98 and
+// the first tests of leftLBL / rightLBL): returns the distance D >= 1 from
+// the line to the nearest grid-0 position and whether the line sits left of
+// the subinterval; false when the line is near, inside or beyond the cutoff.
+__device__ __forceinline__ bool far_line(double nu, double s, double se, double cut, double &D,
+                                         bool &left) {
+  if (nu < s) {
+    D = -(nu - s);
+    left = true;
+    return !(D > cut) && !(D < 1.0);
+  }
+  if (nu > se) {
+    D = (nu - s) - DELTA_WV;
+    left = false;
+    return !(D >= cut) && !(D < 1.0);
+  }
+  return false;
+}
+
+// First grid-0 position index k (0..21) whose distance D + k/2 passes the
+// chi-factor boundary b (strictly when `strict`), decided in double.
+__device__ __forceinline__ int first_k_past(double D, double b, bool strict) {
+  int k = (int)ceil(2.0 * (b - D));
+  k = k < 0 ? 0 : (k > NFAR ? NFAR : k);
+  auto past = [&](int kk) { double d = D + 0.5 * kk; return strict ? (d > b) : (d >= b); };
+  while (k > 0 && past(k - 1)) --k;
+  while (k < NFAR && !past(k)) ++k;
+  return k;
+}
+
+template <int CHI>
+struct ChiPieces {
+  // piece boundaries, strictness, per-piece factor c and exponent rate r
+  // (chi = c * 2^(r * d)); piece 0 is chi = 1.
+  int nb;
+  double b[3];
+  bool strict[3];
+  float c[4], r[4];
+  __device__ ChiPieces(const LevelConst &lv) {
+    const float L2E = 1.4426950408889634f;
+    c[0] = 1.f; r[0] = 0.f;
+    if (CHI == CHI_TONKOV) {
+      nb = 3; b[0] = 3.0; b[1] = 150.0; b[2] = 300.0;
+      strict[0] = strict[1] = strict[2] = true;
+      c[1] = 1.084f; r[1] = -0.027f * L2E;
+      c[2] = 0.208f; r[2] = -0.016f * L2E;
+      c[3] = 0.025f; r[3] = -0.009f * L2E;
+    } else if (CHI == CHI_POLLACK) {
+      nb = 2; b[0] = 3.0; b[1] = 10.0; b[2] = 1e300;
+      strict[0] = strict[1] = strict[2] = false;
+      c[1] = 1.35f; r[1] = -L2E / 10.f;
+      c[2] = 0.614f; r[2] = -L2E / 47.f;
+      c[3] = 0.f; r[3] = 0.f;
+    } else if (CHI == CHI_PERRIN) {
+      nb = 3; b[0] = 3.0; b[1] = 30.0; b[2] = 120.0;
+      strict[0] = true; strict[1] = strict[2] = false;
+      const double b1 = lv.perrin_b1, b2 = lv.perrin_b2, b3 = 0.0232;
+      c[1] = (float)exp(3.0 * b1); r[1] = (float)(-b1 * 1.4426950408889634);
+      c[2] = (float)exp(-27.0 * b1 + 30.0 * b2); r[2] = (float)(-b2 * 1.4426950408889634);
+      c[3] = (float)exp(-27.0 * b1 - 90.0 * b2 + 120.0 * b3); r[3] = (float)(-b3 * 1.4426950408889634);
+    } else {
+      nb = 0; b[0] = b[1] = b[2] = 1e300;
+      strict[0] = strict[1] = strict[2] = true;
+      c[1] = c[2] = c[3] = 1.f; r[1] = r[2] = r[3] = 0.f;
+    }
+  }
+};
+
+template <bool F64, int CHI>
+__global__ void __launch_bounds__(256) far_kernel(FarParams p) {
+  const int item = blockIdx.x;
+  const int l = item / p.n_chunks;
+  const int ci = item - l * p.n_chunks;
+  const int sub = p.chunk_sub[ci];
+  const int64_t begin = p.chunk_begin[ci], end = p.chunk_end[ci];
+  const double s = p.win.sub_s[sub], se = p.win.sub_e[sub], cut = p.cutoff;
+  const LevelConst lv = p.lv[l];
+  const size_t lo = (size_t)l * p.n_lines;
+  double res[NFAR];
+  if (F64) {
+    double acc[NFAR];
+#pragma unroll
+    for (int k = 0; k < NFAR; ++k) acc[k] = 0.0;
+    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+      double D;
+      bool left;
+      if (!far_line(p.nus[lo + i], s, se, cut, D, left)) continue;
+      const Hot64 h = p.hot64[lo + i];
+      if (p.shape == 0 && D * h.qx >= 15.0) {
+        // every position in Lorentz region 0: gamma S / (pi (d^2 + gamma^2)) chi(d)
+#pragma unroll
+        for (int k = 0; k < NFAR; ++k) {
+          const double d = D + 0.5 * k;
+          double f = h.lorA / fma(d, d, h.g2);
+          if (CHI != CHI_NONE) f *= chi_factor_d<CHI>(d, lv);
+          if (left) acc[k] += f; else acc[NFAR - 1 - k] += f;
+        }
+      } else {
+        // some position outside region 0 (or a diagnostic shape): general
+        // shape per position into a local buffer, then static accumulation
+        const LineGen g = p.gen[lo + i];
+        double F[NFAR];
+#pragma unroll 1
+        for (int k = 0; k < NFAR; ++k) {
+          const double d = D + 0.5 * k;
+          if (p.shape == 100) F[k] = 1.0;
+          else if (p.shape == 101) F[k] = d;
+          else F[k] = voigt_general<double, CHI>(d, g, lv, p.c, 1.0);
+        }
+        if (left) {
+#pragma unroll
+          for (int k = 0; k < NFAR; ++k) acc[k] += F[k];
+        } else {
+#pragma unroll
+          for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k] += F[k];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NFAR; ++k) res[k] = acc[k];
+  } else {
+    Kahan acc[NFAR];
+#pragma unroll
+    for (int k = 0; k < NFAR; ++k) acc[k].init();
+    const ChiPieces<CHI> pc(lv);
+    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+      double D;
+      bool left;
+      if (!far_line(p.nus[lo + i], s, se, cut, D, left)) continue;
+      const Hot32 h = p.hot32[lo + i];
+      if (p.shape == 0 && D * h.qx >= 15.0) {
+        // Exact split of the double distance: D = N*2^-11 + f, so that
+        // d_k = (N*2^-11 + k/2) + f is one correctly rounded float.
+        const double Nd = floor(D * 2048.0);
+        const float Nf = (float)(Nd * (1.0 / 2048.0));
+        const float ff = (float)(D - Nd * (1.0 / 2048.0));
+        if (CHI == CHI_NONE) {
+          float F[NFAR];
+#pragma unroll
+          for (int k = 0; k < NFAR; ++k) {
+            const float d = __fadd_rn(Nf + 0.5f * k, ff);
+            F[k] = h.lorA * rcp_approx(fmaf(d, d, h.g2));
+          }
+          if (left) {
+#pragma unroll
+            for (int k = 0; k < NFAR; ++k) acc[k].add(F[k]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k].add(F[k]);
+          }
+        } else {
+          int kb[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) kb[j] = j < pc.nb ? first_k_past(D, pc.b[j], pc.strict[j]) : NFAR;
+          float F[NFAR];
+          if (kb[0] == 0 && kb[1] == NFAR) { // one chi piece over the whole line
+            const float cA = h.lorA * pc.c[1], r = pc.r[1];
+#pragma unroll
+            for (int k = 0; k < NFAR; ++k) {
+              const float d = __fadd_rn(Nf + 0.5f * k, ff);
+              F[k] = (cA * rcp_approx(fmaf(d, d, h.g2))) * ex2_approx(r * d);
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < NFAR; ++k) {
+              const float d = __fadd_rn(Nf + 0.5f * k, ff);
+              const int pcs = (k >= kb[0]) + (k >= kb[1]) + (k >= kb[2]);
+              const float cc = pcs == 0 ? pc.c[0] : (pcs == 1 ? pc.c[1] : (pcs == 2 ? pc.c[2] : pc.c[3]));
+              const float rr = pcs == 0 ? pc.r[0] : (pcs == 1 ? pc.r[1] : (pcs == 2 ? pc.r[2] : pc.r[3]));
+              F[k] = (h.lorA * cc * rcp_approx(fmaf(d, d, h.g2))) * ex2_approx(rr * d);
+            }
+          }
+          if (left) {
+#pragma unroll
+            for (int k = 0; k < NFAR; ++k) acc[k].add(F[k]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k].add(F[k]);
+          }
+        }
+      } else {
+        const LineGen g = p.gen[lo + i];
+        float F[NFAR];
+#pragma unroll 1
+        for (int k = 0; k < NFAR; ++k) {
+          const double d = D + 0.5 * k;
+          if (p.shape == 100) F[k] = 1.f;
+          else if (p.shape == 101) F[k] = (float)d;
+          else F[k] = voigt_general<float, CHI>(d, g, lv, p.c, p.sscale);
+        }
+        if (left) {
+#pragma unroll
+          for (int k = 0; k < NFAR; ++k) acc[k].add(F[k]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k].add(F[k]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NFAR; ++k) res[k] = acc[k].value();
+  }
+  block_reduce_store<NFAR>(res, p.out + ((size_t)l * p.n_chunks + ci) * NFAR);
+}
+
+// --------------------------------------------------------------- near lines
+// First p in [lo, hi) with pred(p), for pred monotone (false ... true),
+// searched by galloping from lo.
+template <class Pred>
+__device__ __forceinline__ int64_t gallop_lb(int64_t lo, int64_t hi, Pred pred) {
+  if (lo >= hi || pred(lo)) return lo;
+  int64_t base = lo, step = 1;
+  while (base + step < hi && !pred(base + step)) {
+    base += step;
+    step <<= 1;
+  }
+  int64_t a = base + 1, b = base + step < hi ? base + step : hi;
+  while (a < b) {
+    const int64_t m = (a + b) >> 1;
+    if (pred(m)) b = m; else a = m + 1;
+  }
+  return a;
+}
+
+template <bool F64>
+struct Acc;
+template <>
+struct Acc<true> {
+  double v;
+  __device__ void init() { v = 0.0; }
+  __device__ void add(double x) { v += x; }
+  __device__ double value() const { return v; }
+};
+template <>
+struct Acc<false> {
+  Kahan k;
+  __device__ void init() { k.init(); }
+  __device__ void add(float x) { k.add(x); }
+  __device__ double value() const { return k.value(); }
+};
+
+template <bool F64, int CHI>
+struct Near {
+  using Real = typename std::conditional<F64, double, float>::type;
+  const double *snu;
+  const int *sidx;
+  const LineGen *gen;
+  LevelConst lv;
+  Consts c;
+  double s, se, cut, sscale;
+  int64_t wlo, whi;
+  int shape;
+  int64_t a, c0, c1, b; // near-left [a, c0), centre [c0, c1), near-right [c1, b)
+
+  __device__ double uu(int64_t q) const { return snu[q] - s; }
+  __device__ bool in_window(int64_t q) const {
+    const int64_t i = sidx[q];
+    return i >= wlo && i < whi;
+  }
+  __device__ Real eval(int64_t q, double X) const {
+    if (shape == 100) return (Real)1;
+    if (shape == 101) return (Real)fabs(X);
+    const LineGen g = gen[sidx[q]];
+    return voigt_general<Real, CHI>(X, g, lv, c, F64 ? 1.0 : sscale);
+  }
+  // centre lines: first q with UU >= x;  first q with V = 10 - UU < y
+  __device__ int64_t lb_uu(int64_t from, double x) const {
+    return gallop_lb(from, c1, [&](int64_t q) { return uu(q) >= x; });
+  }
+  __device__ int64_t lb_v(int64_t from, double y) const {
+    return gallop_lb(from, c1, [&](int64_t q) { return DELTA_WV - uu(q) < y; });
+  }
+};
+
+// upper end of the UU (or V) interval of centre lines that walk over cell j
+// of grid k: (2*floor((j+1)/2) + 2) * H_k  (derived from LineGridCalc.f90:202-331)
+__device__ __forceinline__ double walk_hi(int j, double hk) { return (double)(2 * ((j + 1) / 2) + 2) * hk; }
+
+template <bool F64, int CHI>
+__device__ void fine_grid0_site(const Near<F64, CHI> &nr, int site, void *scr) {
+  const int lane = threadIdx.x & 31;
+  Acc<F64> lo, hi;
+  lo.init();
+  hi.init();
+  const bool edge = site <= 10;
+  const int e = site;       // edge position
+  const int m = site - 10;  // mid index 1..10
+  for (int64_t q = nr.a + lane; q < nr.b; q += 32) {
+    if (!nr.in_window(q)) continue;
+    const double nu = nr.snu[q];
+    double X = 0.0;
+    bool toLo = false, toHi = false;
+    if (nu < nr.s) { // near-left (D < 1): leftLBL grid-0 cells 2..10 and RK(1)
+      const double UU = nu - nr.s;
+      if (-UU > nr.cut) continue;
+      if (edge) {
+        if (e == 0) { toLo = true; X = UU; }
+        else if (e == 1) { toHi = true; X = UU - 1.0; }
+        else { toLo = true; toHi = e <= 9; X = UU - (double)e; }
+      } else if (m >= 2) {
+        toLo = true;
+        X = (UU - (double)(m - 1)) - 0.5;
+      }
+    } else if (nu > nr.se) { // near-right (U < 1): rightLBL grid-0 cells 9..1, RK(1)
+      const double U = (nu - nr.s) - DELTA_WV;
+      if (U >= nr.cut) continue;
+      if (edge) {
+        if (e == 0) { toLo = toHi = true; X = U + 10.0; }
+        else if (e <= 8) { toLo = toHi = true; X = U + (double)(10 - e); }
+        else if (e == 9) { toLo = true; X = U + 1.0; }
+      } else if (m <= 9) {
+        toLo = true;
+        X = (U + (double)(10 - m)) + 0.5;
+      }
+    } else { // centre line: centerLBL grid-0 walks and RK(1)
+      const double UU = nu - nr.s;
+      if (UU >= DELTA_WV) continue;
+      const double V = DELTA_WV - UU;
+      if (edge) {
+        if (e == 0) {
+          toLo = true;
+          toHi = UU >= 2.0;
+          X = UU;
+        } else if (UU >= (double)(e + 1)) { // left walk reached cell e
+          toLo = true;
+          toHi = UU >= (double)(e + 2);
+          X = UU - (double)e;
+        } else if (V >= (double)(11 - e)) { // right walk reached cell e+1
+          toHi = e <= 9;
+          toLo = V >= (double)(12 - e);
+          X = V - (double)(10 - e);
+        }
+      } else {
+        if (UU >= (double)(m + 1)) { toLo = true; X = (UU - (double)m) + 0.5; }
+        else if (V >= (double)(12 - m)) { toLo = true; X = (V - (double)(11 - m)) + 0.5; }
+      }
+    }
+    if (!(toLo || toHi)) continue;
+    const auto f = nr.eval(q, X);
+    if (toLo) lo.add(f);
+    if (toHi) hi.add(f);
+  }
+  double vl = lo.value(), vh = hi.value();
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    vl += __shfl_down_sync(0xffffffffu, vl, off);
+    vh += __shfl_down_sync(0xffffffffu, vh, off);
+  }
+  if (lane == 0) {
+    using Real = typename Near<F64, CHI>::Real;
+    Real *o = (Real *)scr;
+    if (edge) {
+      o[e == 0 ? 0 : 21 + e - 1] = (Real)vl;            // RK(1) or L(e)
+      if (e <= 9) o[1 + e] = (Real)vh;                   // P(e+1)
+    } else {
+      o[11 + m - 1] = (Real)vl;                          // M(m)
+    }
+  }
+}
+
+// One edge site e of grid k (1..9): L(e) and P(e+1).
+template <bool F64, int CHI>
+__device__ void fine_edge_site(const Near<F64, CHI> &nr, int k, int e, int64_t &curL, int64_t &curR,
+                               void *scr) {
+  using Real = typename Near<F64, CHI>::Real;
+  const double hk = h_k(k), hk1 = h_k(k - 1);
+  const int ntk = nt_k(k);
+  Acc<F64> aL, aP;
+  aL.init();
+  aP.init();
+  const bool hasL = e >= 1, hasP = e <= ntk - 1;
+  // centre lines, left walk: UU in [(e+1)hk, walk_hi(e)) -> L(e); [(e+2)hk, walk_hi(e+1)) -> P(e+1)
+  {
+    const double xl0 = (double)(e + 1) * hk, xp0 = (double)(e + 2) * hk;
+    const double xlh = walk_hi(e, hk), xph = walk_hi(e + 1, hk);
+    const double xlo = hasL ? xl0 : xp0;
+    const double xhi = hasL && hasP ? fmax(xlh, xph) : (hasL ? xlh : xph);
+    const int64_t q0 = nr.lb_uu(curL, xlo);
+    curL = q0;
+    for (int64_t q = q0; q < nr.c1; ++q) {
+      const double UU = nr.uu(q);
+      if (UU >= xhi || UU >= DELTA_WV) break;
+      if (!nr.in_window(q)) continue;
+      const bool tl = hasL && UU >= xl0 && UU < xlh;
+      const bool tp = hasP && UU >= xp0 && UU < xph;
+      if (!(tl || tp)) continue;
+      const Real f = nr.eval(q, UU - (double)e * hk);
+      if (tl) aL.add(f);
+      if (tp) aP.add(f);
+    }
+  }
+  // centre lines, right walk: V = 10 - UU; cell j counted r = ntk+1-j from the right
+  {
+    const int rL = ntk + 1 - e, rP = ntk - e;
+    const double yl0 = (double)(rL + 1) * hk, ylh = walk_hi(rL, hk);
+    const double yp0 = (double)(rP + 1) * hk, yph = walk_hi(rP, hk);
+    const double ylo = hasP ? yp0 : yl0;
+    const double yhi = hasL && hasP ? fmax(ylh, yph) : (hasL ? ylh : yph);
+    const int64_t q0 = nr.lb_v(curR, yhi);
+    curR = q0;
+    for (int64_t q = q0; q < nr.c1; ++q) {
+      const double V = DELTA_WV - nr.uu(q);
+      if (V < ylo) break;
+      if (!nr.in_window(q)) continue;
+      const bool tl = hasL && V >= yl0 && V < ylh;
+      const bool tp = hasP && V >= yp0 && V < yph;
+      if (!(tl || tp)) continue;
+      const Real f = nr.eval(q, V - (double)rP * hk);
+      if (tl) aL.add(f);
+      if (tp) aP.add(f);
+    }
+  }
+  // near-left lines (D = -UU < 1): cells 1, 2 of grid k (leftLBL labels 20-28, 121-129)
+  if (e <= 2) {
+    const int64_t q0 = gallop_lb(nr.a, nr.c0, [&](int64_t q) { return nr.uu(q) > -hk1; });
+    for (int64_t q = q0; q < nr.c0; ++q) {
+      if (!nr.in_window(q)) continue;
+      const double UU = nr.uu(q), D = -UU;
+      if (D > nr.cut) continue;
+      const bool own = D >= hk; // H_k <= D < H_{k-1}: cells 1 and 2 of this grid
+      double X;
+      bool tl = false, tp = false;
+      if (e == 0) { tp = own; X = UU; }
+      else if (e == 1) { tl = own; tp = true; X = UU - hk; }
+      else { tl = true; X = UU - hk1; }
+      if (!(tl || tp)) continue;
+      const Real f = nr.eval(q, X);
+      if (tl) aL.add(f);
+      if (tp) aP.add(f);
+    }
+  }
+  // near-right lines (U < 1): cells ntk, ntk-1 (rightLBL labels 60-69, 131-139)
+  if (e >= ntk - 2) {
+    const int64_t q1 = gallop_lb(nr.c1, nr.b, [&](int64_t q) { return (nr.uu(q) - DELTA_WV) >= hk1; });
+    for (int64_t q = nr.c1; q < q1; ++q) {
+      if (!nr.in_window(q)) continue;
+      const double U = nr.uu(q) - DELTA_WV;
+      if (U >= nr.cut) continue;
+      const bool own = U >= hk;
+      double X;
+      bool tl = false, tp = false;
+      if (e == ntk) { tl = own; X = U; }
+      else if (e == ntk - 1) { tp = own; tl = true; X = U + hk; }
+      else { tp = true; X = U + hk1; }
+      if (!(tl || tp)) continue;
+      const Real f = nr.eval(q, X);
+      if (tl) aL.add(f);
+      if (tp) aP.add(f);
+    }
+  }
+  Real *o = (Real *)scr;
+  const int cb = base_k(k) - NT0;
+  if (hasL) o[SCR_FINE_L + cb + e - 1] = (Real)aL.value();
+  if (hasP) o[SCR_FINE_P + cb + e] = (Real)aP.value();
+}
+
+// One mid site m of grid k (1..9): M(m).
+template <bool F64, int CHI>
+__device__ void fine_mid_site(const Near<F64, CHI> &nr, int k, int m, int64_t &curL, int64_t &curR,
+                              void *scr) {
+  using Real = typename Near<F64, CHI>::Real;
+  const double hk = h_k(k), hk1 = h_k(k - 1);
+  const double hn = h_k(k + 1); // H_{k+1}; grid 9 writes H+H, the same number
+  const int ntk = nt_k(k);
+  Acc<F64> aM;
+  aM.init();
+  {
+    const double x0 = (double)(m + 1) * hk, xh = walk_hi(m, hk);
+    const int64_t q0 = nr.lb_uu(curL, x0);
+    curL = q0;
+    for (int64_t q = q0; q < nr.c1; ++q) {
+      const double UU = nr.uu(q);
+      if (UU >= xh || UU >= DELTA_WV) break;
+      if (!nr.in_window(q)) continue;
+      aM.add(nr.eval(q, (UU - (double)m * hk) + hn));
+    }
+  }
+  {
+    const int r = ntk + 1 - m;
+    const double y0 = (double)(r + 1) * hk, yh = walk_hi(r, hk);
+    const int64_t q0 = nr.lb_v(curR, yh);
+    curR = q0;
+    for (int64_t q = q0; q < nr.c1; ++q) {
+      const double V = DELTA_WV - nr.uu(q);
+      if (V < y0) break;
+      if (!nr.in_window(q)) continue;
+      aM.add(nr.eval(q, (V - (double)r * hk) + hn));
+    }
+  }
+  if (m <= 2) {
+    const int64_t q0 = gallop_lb(nr.a, nr.c0, [&](int64_t q) { return nr.uu(q) > -hk1; });
+    for (int64_t q = q0; q < nr.c0; ++q) {
+      if (!nr.in_window(q)) continue;
+      const double UU = nr.uu(q), D = -UU;
+      if (D > nr.cut) continue;
+      if (m == 1) {
+        if (D >= hk) aM.add(nr.eval(q, UU - hn));
+      } else {
+        aM.add(nr.eval(q, (UU - hk) - hn));
+      }
+    }
+  }
+  if (m >= ntk - 1) {
+    const int64_t q1 = gallop_lb(nr.c1, nr.b, [&](int64_t q) { return (nr.uu(q) - DELTA_WV) >= hk1; });
+    for (int64_t q = nr.c1; q < q1; ++q) {
+      if (!nr.in_window(q)) continue;
+      const double U = nr.uu(q) - DELTA_WV;
+      if (U >= nr.cut) continue;
+      if (m == ntk) {
+        if (U >= hk) aM.add(nr.eval(q, U + hn));
+      } else {
+        aM.add(nr.eval(q, (U + hk) + hn));
+      }
+    }
+  }
+  Real *o = (Real *)scr;
+  o[SCR_FINE_M + base_k(k) - NT0 + m - 1] = (Real)aM.value();
+}
+
+// One finest point i (2..NT): direct contributions to RK(i).
+template <bool F64, int CHI>
+__device__ void fine_point_site(const Near<F64, CHI> &nr, int i, int64_t &curL, int64_t &curR,
+                                void *scr) {
+  using Real = typename Near<F64, CHI>::Real;
+  const double H = HSTEP, H9 = h_k(9);
+  const double xi = (double)(i - 1) * H;
+  Acc<F64> a;
+  a.init();
+  // centre lines, left fine loop (LineGridCalc.f90:332-339):
+  // UU in [(i-1)H, (4q+8)H), q = (i-2)/4
+  const double xh = (double)(4 * ((i - 2) / 4) + 8) * H;
+  const int64_t qa = nr.lb_uu(curL, xi);
+  curL = qa;
+  for (int64_t q = qa; q < nr.c1; ++q) {
+    const double UU = nr.uu(q);
+    if (UU >= xh || UU >= DELTA_WV) break;
+    if (!nr.in_window(q)) continue;
+    a.add(nr.eval(q, UU - xi));
+  }
+  // centre lines, right fine loop (LineGridCalc.f90:485-490):
+  // UU < (i-1)H and V < H9 ((NT-i)/4 + 2)
+  const double yv = (double)((NT - i) / 4 + 2) * H9;
+  const int64_t qb = nr.lb_v(curR, yv);
+  curR = qb;
+  for (int64_t q = qb; q < qa; ++q) {
+    if (!nr.in_window(q)) continue;
+    a.add(nr.eval(q, nr.uu(q) - xi));
+  }
+  // near-left lines with D < H9 (leftLBL label 29)
+  if (i <= 5) {
+    const int64_t q0 = gallop_lb(nr.a, nr.c0, [&](int64_t q) { return nr.uu(q) > -H9; });
+    for (int64_t q = q0; q < nr.c0; ++q) {
+      if (!nr.in_window(q)) continue;
+      const double UU = nr.uu(q);
+      if (-UU > nr.cut) continue;
+      const double X = i == 2 ? UU - H : (i == 3 ? (UU - H) - H : (i == 4 ? (UU + H) - H9 : UU - H9));
+      a.add(nr.eval(q, X));
+    }
+  }
+  // near-right lines with U < H9 (rightLBL label 69)
+  if (i >= NT - 3) {
+    const int64_t q1 = gallop_lb(nr.c1, nr.b, [&](int64_t q) { return (nr.uu(q) - DELTA_WV) >= H9; });
+    for (int64_t q = nr.c1; q < q1; ++q) {
+      if (!nr.in_window(q)) continue;
+      const double U = nr.uu(q) - DELTA_WV;
+      if (U >= nr.cut) continue;
+      const double X = i == NT ? U : (i == NT - 1 ? U + H : (i == NT - 2 ? (U + H) + H : (U + H9) - H));
+      a.add(nr.eval(q, X));
+    }
+  }
+  Real *o = (Real *)scr;
+  o[SCR_RK + i - 2] = (Real)a.value();
+}
+
+// site families of phase 2: grid k edges (k=1..9), grid k mids, finest points
+__device__ __forceinline__ void family_of(int f, int &kind, int &k, int &n) {
+  if (f < 9) { kind = 0; k = f + 1; n = nt_k(k) + 1; }
+  else if (f < 18) { kind = 1; k = f - 8; n = nt_k(k); }
+  else { kind = 2; k = 0; n = NT - 1; }
+}
+
+constexpr int FINE_RUN = 8;
+
+template <bool F64, int CHI>
+__global__ void __launch_bounds__(256) fine_kernel(FineParams p) {
+  using Real = typename Near<F64, CHI>::Real;
+  const int u = p.unit0 + blockIdx.x;
+  const int l = u / p.win.n_sub, sub = u - l * p.win.n_sub;
+  __shared__ int64_t sb[4];
+  Near<F64, CHI> nr;
+  nr.snu = p.snu + (size_t)l * p.n_lines;
+  nr.sidx = p.sidx + (size_t)l * p.n_lines;
+  nr.gen = p.gen + (size_t)l * p.n_lines;
+  nr.lv = p.lv[l];
+  nr.c = p.c;
+  nr.s = p.win.sub_s[sub];
+  nr.se = p.win.sub_e[sub];
+  nr.cut = p.cutoff;
+  nr.sscale = p.sscale;
+  nr.wlo = p.win.lo[sub];
+  nr.whi = p.win.hi[sub];
+  nr.shape = p.shape;
+  if (threadIdx.x < 4) {
+    // [a, c0): near-left; [c0, c1): centre; [c1, b): near-right.
+    const int64_t n = p.n_lines;
+    const double s = nr.s, se = nr.se;
+    int64_t r;
+    auto bs = [&](auto pred) {
+      int64_t lo = 0, hi = n;
+      while (lo < hi) {
+        int64_t m = (lo + hi) >> 1;
+        if (pred(m)) hi = m; else lo = m + 1;
+      }
+      return lo;
+    };
+    const double *a = nr.snu;
+    if (threadIdx.x == 0) r = bs([&](int64_t q) { return !(a[q] < s && (a[q] - s) <= -1.0); });
+    else if (threadIdx.x == 1) r = bs([&](int64_t q) { return a[q] >= s; });
+    else if (threadIdx.x == 2) r = bs([&](int64_t q) { return a[q] > se; });
+    else r = bs([&](int64_t q) { return a[q] > se && ((a[q] - s) - DELTA_WV) >= 1.0; });
+    sb[threadIdx.x] = r;
+  }
+  __syncthreads();
+  nr.a = sb[0];
+  nr.c0 = sb[1];
+  nr.c1 = sb[2];
+  nr.b = sb[3];
+  Real *scr = (Real *)p.scratch + (size_t)blockIdx.x * SCR_STRIDE;
+
+  // phase 1: grid-0 sites, one warp each
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int site = warp; site < 21; site += nwarps) fine_grid0_site<F64, CHI>(nr, site, scr);
+
+  // phase 2: runs of FINE_RUN consecutive sites of one family per thread
+  int runs_total = 0;
+  for (int f = 0; f < 19; ++f) {
+    int kind, k, n;
+    family_of(f, kind, k, n);
+    runs_total += (n + FINE_RUN - 1) / FINE_RUN;
+  }
+  for (int r = threadIdx.x; r < runs_total; r += blockDim.x) {
+    int f = 0, base = 0, kind = 0, k = 0, n = 0;
+    for (; f < 19; ++f) {
+      family_of(f, kind, k, n);
+      const int nr_f = (n + FINE_RUN - 1) / FINE_RUN;
+      if (r < base + nr_f) break;
+      base += nr_f;
+    }
+    const int first = (r - base) * FINE_RUN;
+    const int last = min(first + FINE_RUN, n);
+    int64_t curL = nr.c0, curR = nr.c0;
+    for (int t = first; t < last; ++t) {
+      if (kind == 0) fine_edge_site<F64, CHI>(nr, k, t, curL, curR, scr);
+      else if (kind == 1) fine_mid_site<F64, CHI>(nr, k, t + 1, curL, curR, scr);
+      else fine_point_site<F64, CHI>(nr, t + 2, curL, curR, scr);
+    }
+  }
+}
+
+// ----------------------------------------------------------------- cascade
+// interpolation_step (Grids.f90:80-102): quarter-point value of a coarse
+// cell, with the reference's clamp to the half sum.
+__device__ __forceinline__ double quarter(double near_edge, double mid, double far_edge) {
+  double A = 0.375 * near_edge + 0.75 * mid - 0.125 * far_edge;
+  if (A < near_edge || A < mid) A = 0.5 * (near_edge + mid);
+  return A;
+}
+
+template <bool F64>
+__global__ void __launch_bounds__(256) cascade_kernel(CascadeParams p) {
+  using Real = typename std::conditional<F64, double, float>::type;
+  const int ub = blockIdx.x / NT0;        // unit within the batch
+  const int J = blockIdx.x - ub * NT0 + 1; // grid-0 cell of this subtree
+  const int u = p.unit0 + ub;
+  const int l = u / p.n_sub, sub = u - l * p.n_sub;
+  const Real *scr = (const Real *)p.scratch + (size_t)ub * SCR_STRIDE;
+  const double inv = p.inv_sscale;
+  __shared__ double bufA[512 * 3];
+  __shared__ double bufB[512 * 3];
+  __shared__ float outb[2048];
+  __shared__ double rk1;
+  if (threadIdx.x == 0) {
+    // grid-0 cell J: far-line sums over this subinterval's chunks + near part
+    const double *far = p.far + ((size_t)l * p.n_chunks) * NFAR;
+    double fP = 0.0, fM = 0.0, fL = 0.0, f0 = 0.0;
+    for (int c = p.sub_chunk0[sub]; c < p.sub_chunk0[sub + 1]; ++c) {
+      fP += far[(size_t)c * NFAR + 2 * (J - 1)];
+      fM += far[(size_t)c * NFAR + 2 * J - 1];
+      fL += far[(size_t)c * NFAR + 2 * J];
+      f0 += far[(size_t)c * NFAR];
+    }
+    bufA[0] = (fP + (double)scr[1 + J - 1]) * inv;
+    bufA[1] = (fM + (double)scr[11 + J - 1]) * inv;
+    bufA[2] = (fL + (double)scr[21 + J - 1]) * inv;
+    rk1 = (f0 + (double)scr[0]) * inv;
+  }
+  __syncthreads();
+  double *prev = bufA, *cur = bufB;
+  for (int k = 1; k <= 9; ++k) {
+    const int ncell = 1 << k;
+    const int cb = base_k(k) - NT0 + (J - 1) * ncell;
+    for (int t = threadIdx.x; t < ncell; t += blockDim.x) {
+      const int pt = t >> 1;
+      const double cP = prev[3 * pt], cM = prev[3 * pt + 1], cL = prev[3 * pt + 2];
+      double P = (double)scr[SCR_FINE_P + cb + t] * inv;
+      double M = (double)scr[SCR_FINE_M + cb + t] * inv;
+      double L = (double)scr[SCR_FINE_L + cb + t] * inv;
+      if ((t & 1) == 0) { // finer cell 2J-1
+        P += cP; M += quarter(cP, cM, cL); L += cM;
+      } else {            // finer cell 2J
+        P += cM; M += quarter(cL, cM, cP); L += cL;
+      }
+      cur[3 * t] = P;
+      cur[3 * t + 1] = M;
+      cur[3 * t + 2] = L;
+    }
+    __syncthreads();
+    double *tmp = prev; prev = cur; cur = tmp;
+  }
+  // grid 9 -> finest points RK(4j-2 .. 4j+1), j = grid-9 cell (Grids.f90:121-138)
+  const double dens = p.target == 1 ? p.lv[l].density : 1.0;
+  const size_t rec = ((size_t)(p.level_out0 + l) * p.n_sub + sub) * NT;
+  for (int t = threadIdx.x; t < 512; t += blockDim.x) {
+    const double cP = prev[3 * t], cM = prev[3 * t + 1], cL = prev[3 * t + 2];
+    const int j = (J - 1) * 512 + t + 1;
+    const double v[4] = {quarter(cP, cM, cL), cM, quarter(cL, cM, cP), cL};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = 4 * j - 2 + q; // RK index, 1-based
+      const double x = ((double)scr[SCR_RK + i - 2] * inv + v[q]) * dens;
+      outb[4 * t + q] = (float)x;
+      if (p.out64) p.out64[rec + i - 1] = x;
+    }
+  }
+  if (J == 1 && threadIdx.x == 0) {
+    const double x = rk1 * dens;
+    p.out[rec] = (float)x;
+    if (p.out64) p.out64[rec] = x;
+  }
+  __syncthreads();
+  // coalesced write of RK((J-1)*2048+2 .. J*2048+1), 128-bit stores where aligned
+  float *dst = p.out + rec + (size_t)(J - 1) * 2048 + 1;
+  const int head = (int)((4 - (((uintptr_t)dst >> 2) & 3)) & 3);
+  if ((int)threadIdx.x < head) dst[threadIdx.x] = outb[threadIdx.x];
+  const int nvec = (2048 - head) >> 2;
+  float4 *dv = (float4 *)(dst + head);
+  for (int t = threadIdx.x; t < nvec; t += blockDim.x) {
+    const int o = head + 4 * t;
+    dv[t] = make_float4(outb[o], outb[o + 1], outb[o + 2], outb[o + 3]);
+  }
+  const int tail0 = head + 4 * nvec;
+  if ((int)threadIdx.x < 2048 - tail0) dst[tail0 + threadIdx.x] = outb[tail0 + threadIdx.x];
+}
+
+// Raw accumulators of one unit in the oracle's layout (diagnostics).
+template <bool F64>
+__global__ void dump_kernel(CascadeParams p) {
+  using Real = typename std::conditional<F64, double, float>::type;
+  const int ub = p.dump_unit - p.unit0;
+  const int u = p.dump_unit;
+  const int l = u / p.n_sub, sub = u - l * p.n_sub;
+  const Real *scr = (const Real *)p.scratch + (size_t)ub * SCR_STRIDE;
+  const double inv = p.inv_sscale;
+  const double *far = p.far + ((size_t)l * p.n_chunks) * NFAR;
+  double *d = p.dump;
+  for (int t = threadIdx.x; t < NT + 3 * NCELLS; t += blockDim.x) d[t] = 0.0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < NFAR + 1; t += blockDim.x) {
+    double fs = 0.0;
+    if (t < NFAR)
+      for (int c = p.sub_chunk0[sub]; c < p.sub_chunk0[sub + 1]; ++c) fs += far[(size_t)c * NFAR + t];
+    if (t == 0) d[0] = (fs + (double)scr[0]) * inv;               // RK(1)
+    if (t < NFAR && (t & 1) == 0) {                              // integer position e
+      const int e = t / 2;
+      if (e <= 9) d[NT + e] = (fs + (double)scr[1 + e]) * inv;    // P(e+1)
+      if (e >= 1) d[NT + 2 * NCELLS + e - 1] = (fs + (double)scr[21 + e - 1]) * inv; // L(e)
+    } else if (t < NFAR) {                                       // mid of cell m
+      const int m = (t + 1) / 2;
+      d[NT + NCELLS + m - 1] = (fs + (double)scr[11 + m - 1]) * inv;
+    }
+  }
+  for (int t = threadIdx.x; t < NFINE_CELLS; t += blockDim.x) {
+    d[NT + NT0 + t] = (double)scr[SCR_FINE_P + t] * inv;
+    d[NT + NCELLS + NT0 + t] = (double)scr[SCR_FINE_M + t] * inv;
+    d[NT + 2 * NCELLS + NT0 + t] = (double)scr[SCR_FINE_L + t] * inv;
+  }
+  for (int t = threadIdx.x; t < NT - 1; t += blockDim.x) d[1 + t] = (double)scr[SCR_RK + t] * inv;
+}
+
+// ------------------------------------------------------------ eval count
+// FSHAPE calls of the reference schedule for one line (LineGridCalc.f90).
+__device__ __forceinline__ unsigned count_line(double nu, double s, double se, double cut) {
+  const double H = HSTEP;
+  if (nu < s) {
+    const double D = -(nu - s);
+    if (D > cut) return 0;
+    if (!(D < 1.0)) return 21;
+    for (int k = 1; k <= 9; ++k)
+      if (!(D < h_k(k))) return 21 + 2 * k;
+    return 41;
+  }
+  if (nu > se) {
+    const double U = (nu - s) - DELTA_WV;
+    if (U >= cut) return 0;
+    if (!(U < 1.0)) return 21;
+    for (int k = 1; k <= 8; ++k)
+      if (!(U < h_k(k))) return 21 + 2 * k;
+    if (!(U < h_k(9))) return 40;
+    return 42;
+  }
+  const double UU = nu - s;
+  if (UU >= DELTA_WV) return 0;
+  unsigned n = 2; // F(0) and F(UU)
+  // left walk: grid k runs when UU >= 2 H_k; I_k = floor(UU/H_k) - 1
+  long long I = 0, cells = 0;
+  if (UU >= H) {
+    for (int k = 0; k <= 9; ++k) {
+      const double hk = h_k(k);
+      if (k > 0) I *= 2;
+      if (UU >= 2.0 * hk) {
+        const long long Ik = (long long)floor(UU / hk) - 1;
+        cells += Ik - I;
+        I = Ik;
+      }
+    }
+    n += (unsigned)(2 * cells) + (unsigned)((long long)floor(UU / H) - 4 * I);
+  }
+  const double V = DELTA_WV - UU;
+  long long III = 0, rc = 0;
+  for (int k = 0; k <= 9; ++k) {
+    const double hk = h_k(k);
+    if (k > 0) III *= 2;
+    if (V >= 2.0 * hk) {
+      const long long Ik = (long long)floor(V / hk) - 1;
+      rc += Ik - III;
+      III = Ik;
+    }
+  }
+  const long long npoint = (long long)floor(UU / H) + 2;
+  n += 1 + (unsigned)(2 * rc) + (unsigned)((NT - 4 * III) - npoint + 1);
+  return n;
+}
+
+__global__ void __launch_bounds__(256) count_kernel(CountParams p) {
+  const int item = blockIdx.x;
+  const int l = item / p.n_chunks;
+  const int ci = item - l * p.n_chunks;
+  const int sub = p.chunk_sub[ci];
+  const double s = p.win.sub_s[sub], se = p.win.sub_e[sub];
+  unsigned long long n = 0, nf = 0;
+  for (int64_t i = p.chunk_begin[ci] + threadIdx.x; i < p.chunk_end[ci]; i += blockDim.x) {
+    const double nu = p.nus[(size_t)l * p.n_lines + i];
+    double D;
+    bool left;
+    n += count_line(nu, s, se, p.cutoff);
+    if (far_line(nu, s, se, p.cutoff, D, left)) nf += NFAR;
+  }
+  __shared__ unsigned long long red[32][2];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    n += __shfl_down_sync(0xffffffffu, n, off);
+    nf += __shfl_down_sync(0xffffffffu, nf, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5][0] = n;
+    red[threadIdx.x >> 5][1] = nf;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0, tf = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      t += red[w][0];
+      tf += red[w][1];
+    }
+    p.out[2 * (size_t)item] = t;
+    p.out[2 * (size_t)item + 1] = tf;
+  }
+}
+
+// --------------------------------------------------------------- launchers
+static bool wiso_loaded = false;
+
+cudaError_t launch_prep(const PrepParams &p, cudaStream_t st) {
+  if (!wiso_loaded) {
+    cudaError_t e = cudaMemcpyToSymbol(c_wiso, MARFA_WISO_D, sizeof(MARFA_WISO_D));
+    if (e != cudaSuccess) return e;
+    wiso_loaded = true;
+  }
+  dim3 grid((unsigned)((p.lines.n + 255) / 256), (unsigned)p.n_levels);
+  prep_kernel<<<grid, 256, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sort(const SortParams &p, cudaStream_t st) {
+  dim3 grid((unsigned)((p.n + 255) / 256), (unsigned)p.n_levels);
+  rank_kernel<<<grid, 256, 0, st>>>(p);
+  scatter_kernel<<<grid, 256, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <bool F64>
+static void far_dispatch(const FarParams &p, int chi, unsigned nblk, cudaStream_t st) {
+  switch (chi) {
+  case CHI_TONKOV: far_kernel<F64, CHI_TONKOV><<<nblk, 256, 0, st>>>(p); break;
+  case CHI_POLLACK: far_kernel<F64, CHI_POLLACK><<<nblk, 256, 0, st>>>(p); break;
+  case CHI_PERRIN: far_kernel<F64, CHI_PERRIN><<<nblk, 256, 0, st>>>(p); break;
+  default: far_kernel<F64, CHI_NONE><<<nblk, 256, 0, st>>>(p); break;
+  }
+}
+
+cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t st) {
+  const unsigned nblk = (unsigned)p.n_chunks * (unsigned)p.n_levels;
+  if (nblk == 0) return cudaSuccess;
+  if (precision == 0) far_dispatch<true>(p, chi, nblk, st);
+  else far_dispatch<false>(p, chi, nblk, st);
+  return cudaGetLastError();
+}
+
+template <bool F64>
+static void fine_dispatch(const FineParams &p, int chi, cudaStream_t st) {
+  switch (chi) {
+  case CHI_TONKOV: fine_kernel<F64, CHI_TONKOV><<<p.n_units, 256, 0, st>>>(p); break;
+  case CHI_POLLACK: fine_kernel<F64, CHI_POLLACK><<<p.n_units, 256, 0, st>>>(p); break;
+  case CHI_PERRIN: fine_kernel<F64, CHI_PERRIN><<<p.n_units, 256, 0, st>>>(p); break;
+  default: fine_kernel<F64, CHI_NONE><<<p.n_units, 256, 0, st>>>(p); break;
+  }
+}
+
+cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st) {
+  if (p.n_units == 0) return cudaSuccess;
+  if (precision == 0) fine_dispatch<true>(p, chi, st);
+  else fine_dispatch<false>(p, chi, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st) {
+  if (p.n_units == 0) return cudaSuccess;
+  const unsigned nblk = (unsigned)p.n_units * NT0;
+  if (precision == 0) cascade_kernel<true><<<nblk, 256, 0, st>>>(p);
+  else cascade_kernel<false><<<nblk, 256, 0, st>>>(p);
+  if (p.dump && p.dump_unit >= p.unit0 && p.dump_unit < p.unit0 + p.n_units) {
+    if (precision == 0) dump_kernel<true><<<1, 256, 0, st>>>(p);
+    else dump_kernel<false><<<1, 256, 0, st>>>(p);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count(const CountParams &p, cudaStream_t st) {
+  const unsigned nblk = (unsigned)p.n_chunks * (unsigned)p.n_levels;
+  if (nblk == 0) return cudaSuccess;
+  count_kernel<<<nblk, 256, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+} // namespace marfa

@@ -1,0 +1,119 @@
+// marfa_kernels.cuh -- launch interface between the host driver and the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "marfa_device.cuh"
+
+namespace marfa {
+
+// SoA copy of the line list (line-index order, index 0 = record 1).
+struct DeviceLines {
+  const double *nu;
+  const float *S, *gair, *gself, *elow, *nair, *delta;
+  const int *iso; // jointMolIso / 100
+  int64_t n;
+};
+
+struct PrepParams {
+  DeviceLines lines;
+  const double *tips; // [n_iso][n_temp]
+  int n_iso, n_temp;
+  const LevelConst *lv; // [Lc]
+  int n_levels;         // Lc
+  Consts c;
+  double sscale;        // 2^scale_exp for the FP32-compensated hot records
+  double *nus;          // [Lc][N]
+  LineGen *gen;         // [Lc][N]
+  Hot32 *hot32;         // [Lc][N] or null
+  Hot64 *hot64;         // [Lc][N] or null
+  int *err;             // device error word (max of status codes)
+};
+
+struct SortParams {
+  const double *nu;     // unshifted, sorted
+  const double *nus;    // [Lc][N]
+  const double *margin; // [Lc] half-width of the re-ordering window
+  int64_t n;
+  int n_levels;
+  int64_t *rank;        // [Lc][N] scratch
+  double *snu;          // [Lc][N] sorted shifted centres
+  int *sidx;            // [Lc][N] line index of each sorted slot
+};
+
+struct WindowTable {
+  const double *sub_s, *sub_e;   // [n_sub] subinterval start / end
+  const int64_t *lo, *hi;        // [n_sub] line window [lo, hi) (0-based)
+  int n_sub;
+};
+
+struct FarParams {
+  const double *nus;
+  const Hot32 *hot32;
+  const Hot64 *hot64;
+  const LineGen *gen;
+  const LevelConst *lv;
+  WindowTable win;
+  const int *chunk_sub;          // [C]
+  const int64_t *chunk_begin, *chunk_end;
+  int n_chunks;                  // C (per level)
+  int n_levels;                  // Lc
+  int64_t n_lines;
+  double cutoff;
+  double sscale;
+  int shape;
+  Consts c;
+  double *out;                   // [Lc][C][NFAR]
+};
+
+struct FineParams {
+  const double *snu;
+  const int *sidx;
+  const LineGen *gen;
+  const LevelConst *lv;
+  WindowTable win;
+  int64_t n_lines;
+  int unit0;                     // first (level-in-chunk * n_sub + sub) of this batch
+  int n_units;
+  double cutoff;
+  double sscale;
+  int shape;
+  Consts c;
+  void *scratch;                 // [n_units][SCR_STRIDE] float or double
+};
+
+struct CascadeParams {
+  const void *scratch;           // from the fine kernel
+  const double *far;             // [Lc][C][NFAR]
+  const int *sub_chunk0;         // [n_sub + 1] first chunk of each subinterval
+  const LevelConst *lv;
+  int n_chunks, n_sub;
+  int unit0, n_units;
+  int level_out0;                // global level index of level-in-chunk 0
+  double inv_sscale;
+  int target;
+  float *out;                    // [levels][n_sub][NT]
+  double *out64;                 // optional
+  double *dump;                  // optional raw-accumulator dump of one unit
+  int dump_unit;
+};
+
+struct CountParams {
+  const double *nus;
+  WindowTable win;
+  const int *chunk_sub;
+  const int64_t *chunk_begin, *chunk_end;
+  int n_chunks, n_levels;
+  int64_t n_lines;
+  double cutoff;
+  unsigned long long *out;       // [Lc][C]
+};
+
+// launchers (marfa_kernels.cu)
+cudaError_t launch_prep(const PrepParams &p, cudaStream_t st);
+cudaError_t launch_sort(const SortParams &p, cudaStream_t st);
+cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t st);
+cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st);
+cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st);
+cudaError_t launch_count(const CountParams &p, cudaStream_t st);
+
+} // namespace marfa
