@@ -47,7 +47,7 @@ struct marfa_ctx {
   int *d_err = nullptr;
   // grow-only work buffers
   DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
-      b_out, b_out64, b_dump, b_count;
+      b_out, b_out64, b_dump, b_count, b_near, b_gstage;
   std::string err;
   std::vector<cudaEvent_t> events;
   // timing marks of the last compute call: (family, start, stop); family 5
@@ -418,22 +418,47 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p;
     const int out_level0 = o.dev_out ? l0 : 0;
     const int units = nl * nsub;
-    for (int u0 = 0; u0 < units; u0 += UB) {
-      const int nu_ = std::min(UB, units - u0);
-      FineParams fn;
-      fn.snu = sp.snu;
-      fn.sidx = sp.sidx;
-      fn.gen = pp.gen;
-      fn.lv = pp.lv;
-      fn.win = win;
-      fn.n_lines = N;
+    // near-line counts of this chunk's units size the fine kernel's staging
+    FineParams fn;
+    fn.snu = sp.snu;
+    fn.sidx = sp.sidx;
+    fn.gen = pp.gen;
+    fn.lv = pp.lv;
+    fn.win = win;
+    fn.n_lines = N;
+    fn.cutoff = run->cutoff;
+    fn.sscale = sscale;
+    fn.shape = run->shape;
+    fn.c = cst;
+    fn.scratch = ctx->b_scr.p;
+    fn.err = ctx->d_err;
+    fn.unit0 = 0;
+    fn.n_units = units;
+    CK(ensure(ctx->b_near, (size_t)units * 4), "alloc near counts");
+    CK(launch_near_count(fn, (int *)ctx->b_near.p, st), "near count kernel");
+    ctx->launches += 1;
+    std::vector<int> ncount(units);
+    CK(cudaMemcpyAsync(ncount.data(), ctx->b_near.p, (size_t)units * 4, cudaMemcpyDeviceToHost, st), "d2h near");
+    CK(cudaStreamSynchronize(st), "sync near");
+    const int max_near = units ? *std::max_element(ncount.begin(), ncount.end()) : 0;
+    const int smem_max = f64 ? 4096 : 5120;
+    fn.smem_cap = std::max(256, std::min(smem_max, (max_near + 255) / 256 * 256));
+    fn.gstage = nullptr;
+    fn.gstage_cap = 0;
+    fn.gstage_bytes = 0;
+    int UBc = UB;
+    if (max_near > fn.smem_cap) {
+      fn.gstage_cap = (max_near + 255) / 256 * 256;
+      fn.gstage_bytes = fine_smem_bytes(fn.gstage_cap, f64);
+      const size_t room = std::max<size_t>(fn.gstage_bytes, (size_t)1 << 30);
+      UBc = (int)std::max<size_t>(1, std::min<size_t>((size_t)UB, room / fn.gstage_bytes));
+      CK(ensure(ctx->b_gstage, (size_t)UBc * fn.gstage_bytes), "alloc staging");
+      fn.gstage = ctx->b_gstage.p;
+    }
+    for (int u0 = 0; u0 < units; u0 += UBc) {
+      const int nu_ = std::min(UBc, units - u0);
       fn.unit0 = u0;
       fn.n_units = nu_;
-      fn.cutoff = run->cutoff;
-      fn.sscale = sscale;
-      fn.shape = run->shape;
-      fn.c = cst;
-      fn.scratch = ctx->b_scr.p;
       cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
       if (f0) cudaEventRecord(f0, st);
       CK(launch_fine(fn, run->precision, chi, st), "fine kernel");
@@ -621,7 +646,7 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
     if (p) cudaFree(p);
   DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
                   &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
-                  &ctx->b_out64, &ctx->b_dump, &ctx->b_count};
+                  &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_near, &ctx->b_gstage};
   for (DevBuf *b : bs) release(*b);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

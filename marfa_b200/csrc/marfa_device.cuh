@@ -163,26 +163,54 @@ __device__ __forceinline__ Real horner(Real x, double c0, Rest... rest) {
 }
 
 // ------------------------------------------------------- general line shape
+// Per-line parameters of the general shape evaluation.  Region decisions use
+// qx and vy in double in both precisions; values are computed in Real.
+template <typename Real>
+struct ShapeP {
+  double qx;   // sqln2 / alpha_D
+  double vy;   // sqln2 * gamma_L / alpha_D
+  Real lorA;   // gamma S / PI (scaled)
+  Real g2;     // gamma^2
+  Real hum;    // S sqln2 / (sqrt(PI) alpha_D) (scaled)
+};
+
+template <typename Real>
+__device__ __forceinline__ ShapeP<Real> shape_params(const LineGen &g, const Consts &c, double sscale) {
+  ShapeP<Real> s;
+  s.qx = g.qx;
+  s.vy = g.vy;
+  s.lorA = (Real)(g.lorA * sscale);
+  s.g2 = (Real)(g.gamma * g.gamma);
+  s.hum = (Real)(g.S * sscale * (c.sqln2 / (c.sqrtpi * g.alpha)));
+  return s;
+}
+
+__device__ __forceinline__ float fast_div(float a, float b) { return a * rcp_approx(b); }
+__device__ __forceinline__ double fast_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float exp_neg(float x) { return ex2_approx(-x * 1.4426950408889634f); }
+__device__ __forceinline__ double exp_neg(double x) { return exp(-x); }
+
 // Humlicek-Kuntz voigt of Shapes.f90:22-133 with the reference's region 0
-// and region-4 asymptotics (Spectroscopy.f90:232-261).  The region is chosen
-// from VX = |X| * qx and VY in double (identical decisions in both
-// precisions); the region's formula runs in Real.  Returns S-scaled shape.
+// and region-4 asymptotics (Spectroscopy.f90:232-261), times the intensity.
+// Region chosen from VX = |X| qx and VY in double; formula in Real.
+//   region 0 / asym1: chi-corrected Lorentz  lorA / (X^2 + gamma^2) * chi
+//   regions 1-3     : Kuntz rational function of VX^2 * hum
+//   asym2           : doppler + gamma S / (PI X^2) (1 + F)
+//   doppler         : hum * exp(-VX^2)
 template <typename Real, int CHI>
-__device__ Real voigt_general(double Xd, const LineGen &g, const LevelConst &lv, const Consts &c,
-                              double sscale) {
+__device__ Real voigt_eval(double Xd, const ShapeP<Real> &p, const LevelConst &lv, double sqrt14) {
   const double ax = fabs(Xd);
-  const double VXd = ax * g.qx;
-  const double VYd = g.vy;
-  const Real S = (Real)(g.S * sscale);
-  if (VXd >= 15.0) { // region 0: chi-corrected Lorentz
-    Real lor = (Real)(g.lorA * sscale) / ((Real)ax * (Real)ax + (Real)g.gamma * (Real)g.gamma);
+  const double VXd = ax * p.qx;
+  const double VYd = p.vy;
+  const Real axr = (Real)ax;
+  if (VXd >= 15.0) { // region 0
+    const Real lor = fast_div(p.lorA, axr * axr + p.g2);
+    if (CHI == CHI_NONE) return lor;
     if (sizeof(Real) == 8) return lor * (Real)chi_factor_d<CHI>(ax, lv);
     return lor * (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
   }
   const Real VX = (Real)VXd, VY = (Real)VYd;
   const Real VXs = VX * VX;
-  // (value) / sqrt(pi) / (alpha / sqln2) * S
-  const Real hum = S * (Real)(c.sqln2 / (c.sqrtpi * g.alpha));
   const double sum = VXd + VYd;
   if (sum >= 15.0) { // region 1
     const Real Y = VY, Y2 = Y * Y;
@@ -190,7 +218,7 @@ __device__ Real voigt_general(double Xd, const LineGen &g, const LevelConst &lv,
     const Real B1 = (Real)0.5641896 * Y;
     const Real A2 = (Real)0.25 + Y2 + Y2 * Y2;
     const Real B2 = Y2 + Y2 - (Real)1.;
-    return (A1 + B1 * VXs) / (A2 + B2 * VXs + VXs * VXs) * hum;
+    return (A1 + B1 * VXs) / (A2 + B2 * VXs + VXs * VXs) * p.hum;
   }
   if (sum >= 5.5) { // region 2
     const Real Y = VY, Y2 = Y * Y;
@@ -203,7 +231,7 @@ __device__ Real voigt_general(double Xd, const LineGen &g, const LevelConst &lv,
     const Real C4 = (Real)10.5 + (Real)6.0 * (Y2 - (Real)1.0) * Y2;
     const Real D4 = (Real)4.0 * Y2 - (Real)6.0;
     return (((D3 * VXs + C3) * VXs + B3) * VXs + A3) /
-           ((((VXs + D4) * VXs + C4) * VXs + B4) * VXs + A4) * hum;
+           ((((VXs + D4) * VXs + C4) * VXs + B4) * VXs + A4) * p.hum;
   }
   if (VXd <= 1.0 || VYd >= 0.02) { // region 3
     const Real Y = VY;
@@ -222,25 +250,32 @@ __device__ Real voigt_general(double Xd, const LineGen &g, const LevelConst &lv,
     const Real D6 = horner<Real>(Y, 10., 53.5952, 92.7586, 55.0293, 22.0353);
     const Real E6 = horner<Real>(Y, 5.0, 13.3988, 1.49645);
     return ((((E5 * VXs + D5) * VXs + C5) * VXs + B5) * VXs + A5) /
-           (((((VXs + E6) * VXs + D6) * VXs + C6) * VXs + B6) * VXs + A6) * hum;
+           (((((VXs + E6) * VXs + D6) * VXs + C6) * VXs + B6) * VXs + A6) * p.hum;
   }
   // region 4
   if (VXd > 5.0) { // voigtAsymptotic1
-    Real lor = (Real)(g.lorA * sscale) / ((Real)ax * (Real)ax + (Real)g.gamma * (Real)g.gamma);
-    Real chi = (sizeof(Real) == 8) ? (Real)chi_factor_d<CHI>(ax, lv) : (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
+    const Real lor = fast_div(p.lorA, axr * axr + p.g2);
+    Real chi = (Real)1;
+    if (CHI != CHI_NONE)
+      chi = (sizeof(Real) == 8) ? (Real)chi_factor_d<CHI>(ax, lv) : (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
     return lor * chi * ((Real)1. + (Real)1.5 / VXs);
   }
-  // doppler = sqln2/(sqrt(pi) alpha) exp(-(X/alpha)^2 ln2) S = hum * exp(-VX^2)
-  const Real dop = hum * (Real)exp(-(VXd * VXd));
-  if (VXd > c.sqrt14) { // voigtAsymptotic2
+  const Real dop = p.hum * exp_neg(VXs);
+  if (VXd > sqrt14) { // voigtAsymptotic2
     const double Ut[9] = {1., 1.5, 2., 2.5, 3., 3.5, 4., 4.5, 5.};
     const double Wt[9] = {-0.688, 0.2667, 0.6338, 0.4405, 0.2529, 0.1601, 0.1131, 0.0853, 0.068};
     int I = (int)(VXd / 0.5 - 1.00001); // 1-based, truncation
     I = I < 1 ? 1 : (I > 8 ? 8 : I);
     const Real F = (Real)(2. * (Wt[I - 1] * (Ut[I] - VXd) + Wt[I] * (VXd - Ut[I - 1])));
-    return dop + (Real)g.gamma / ((Real)c.pi * (Real)(ax * ax)) * ((Real)1. + F) * S;
+    return dop + p.lorA / (axr * axr) * ((Real)1. + F);
   }
   return dop;
+}
+
+template <typename Real, int CHI>
+__device__ __forceinline__ Real voigt_general(double Xd, const LineGen &g, const LevelConst &lv,
+                                              const Consts &c, double sscale) {
+  return voigt_eval<Real, CHI>(Xd, shape_params<Real>(g, c, sscale), lv, c.sqrt14);
 }
 
 } // namespace marfa

@@ -371,16 +371,16 @@ __global__ void __launch_bounds__(256) far_kernel(FarParams p) {
 // First p in [lo, hi) with pred(p), for pred monotone (false ... true),
 // searched by galloping from lo.
 template <class Pred>
-__device__ __forceinline__ int64_t gallop_lb(int64_t lo, int64_t hi, Pred pred) {
+__device__ __forceinline__ int gallop_lb(int lo, int hi, Pred pred) {
   if (lo >= hi || pred(lo)) return lo;
-  int64_t base = lo, step = 1;
+  int base = lo, step = 1;
   while (base + step < hi && !pred(base + step)) {
     base += step;
     step <<= 1;
   }
-  int64_t a = base + 1, b = base + step < hi ? base + step : hi;
+  int a = base + 1, b = base + step < hi ? base + step : hi;
   while (a < b) {
-    const int64_t m = (a + b) >> 1;
+    const int m = (a + b) >> 1;
     if (pred(m)) b = m; else a = m + 1;
   }
   return a;
@@ -391,48 +391,60 @@ struct Acc;
 template <>
 struct Acc<true> {
   double v;
-  __device__ void init() { v = 0.0; }
-  __device__ void add(double x) { v += x; }
-  __device__ double value() const { return v; }
+  __device__ __forceinline__ void init() { v = 0.0; }
+  __device__ __forceinline__ void add(double x) { v += x; }
+  __device__ __forceinline__ double value() const { return v; }
 };
 template <>
 struct Acc<false> {
   Kahan k;
-  __device__ void init() { k.init(); }
-  __device__ void add(float x) { k.add(x); }
-  __device__ double value() const { return k.value(); }
+  __device__ __forceinline__ void init() { k.init(); }
+  __device__ __forceinline__ void add(float x) { k.add(x); }
+  __device__ __forceinline__ double value() const { return k.value(); }
 };
 
-template <bool F64, int CHI>
-struct Near {
+// The lines of one (level, subinterval) that lie within 1 cm-1 of the
+// subinterval or inside it, in shifted-centre order, compacted to those the
+// reference schedule lets contribute (inside the line window, within the
+// cutoff, centre lines with UU < 10).  Held in shared memory (or, for very
+// dense line lists, in a global staging area) as structure of arrays.
+template <bool F64>
+struct NearStore {
   using Real = typename std::conditional<F64, double, float>::type;
-  const double *snu;
-  const int *sidx;
-  const LineGen *gen;
+  double *uu;           // fl(nu' - start)
+  double *qx, *vy;
+  Real *lorA, *g2, *hum;
+  int m, c0, c1;        // near-left [0, c0), centre [c0, c1), near-right [c1, m)
   LevelConst lv;
-  Consts c;
-  double s, se, cut, sscale;
-  int64_t wlo, whi;
-  int shape;
-  int64_t a, c0, c1, b; // near-left [a, c0), centre [c0, c1), near-right [c1, b)
+  double sqrt14;
 
-  __device__ double uu(int64_t q) const { return snu[q] - s; }
-  __device__ bool in_window(int64_t q) const {
-    const int64_t i = sidx[q];
-    return i >= wlo && i < whi;
+  __device__ __forceinline__ Real eval(int q, double X) const {
+    ShapeP<Real> sp;
+    sp.qx = qx[q];
+    sp.vy = vy[q];
+    sp.lorA = lorA[q];
+    sp.g2 = g2[q];
+    sp.hum = hum[q];
+    return sp.qx < 0.0 ? (sp.vy < 0.0 ? (Real)1 : (Real)fabs(X)) // diagnostic shapes
+                       : voigt_eval<Real, 0>(X, sp, lv, sqrt14);
   }
-  __device__ Real eval(int64_t q, double X) const {
-    if (shape == 100) return (Real)1;
-    if (shape == 101) return (Real)fabs(X);
-    const LineGen g = gen[sidx[q]];
-    return voigt_general<Real, CHI>(X, g, lv, c, F64 ? 1.0 : sscale);
+  template <int CHI>
+  __device__ __forceinline__ Real evalc(int q, double X) const {
+    ShapeP<Real> sp;
+    sp.qx = qx[q];
+    sp.vy = vy[q];
+    sp.lorA = lorA[q];
+    sp.g2 = g2[q];
+    sp.hum = hum[q];
+    if (sp.qx < 0.0) return sp.vy < 0.0 ? (Real)1 : (Real)fabs(X);
+    return voigt_eval<Real, CHI>(X, sp, lv, sqrt14);
   }
   // centre lines: first q with UU >= x;  first q with V = 10 - UU < y
-  __device__ int64_t lb_uu(int64_t from, double x) const {
-    return gallop_lb(from, c1, [&](int64_t q) { return uu(q) >= x; });
+  __device__ __forceinline__ int lb_uu(int from, double x) const {
+    return gallop_lb(from, c1, [&](int q) { return uu[q] >= x; });
   }
-  __device__ int64_t lb_v(int64_t from, double y) const {
-    return gallop_lb(from, c1, [&](int64_t q) { return DELTA_WV - uu(q) < y; });
+  __device__ __forceinline__ int lb_v(int from, double y) const {
+    return gallop_lb(from, c1, [&](int q) { return DELTA_WV - uu[q] < y; });
   }
 };
 
@@ -440,147 +452,104 @@ struct Near {
 // of grid k: (2*floor((j+1)/2) + 2) * H_k  (derived from LineGridCalc.f90:202-331)
 __device__ __forceinline__ double walk_hi(int j, double hk) { return (double)(2 * ((j + 1) / 2) + 2) * hk; }
 
+// Grid-0 and RK(1) contributions of one near line: leftLBL grid-0 cells 2..10
+// (near-left), centerLBL walks (centre), rightLBL cells 9..1 (near-right).
 template <bool F64, int CHI>
-__device__ void fine_grid0_site(const Near<F64, CHI> &nr, int site, void *scr) {
-  const int lane = threadIdx.x & 31;
-  Acc<F64> lo, hi;
-  lo.init();
-  hi.init();
-  const bool edge = site <= 10;
-  const int e = site;       // edge position
-  const int m = site - 10;  // mid index 1..10
-  for (int64_t q = nr.a + lane; q < nr.b; q += 32) {
-    if (!nr.in_window(q)) continue;
-    const double nu = nr.snu[q];
-    double X = 0.0;
-    bool toLo = false, toHi = false;
-    if (nu < nr.s) { // near-left (D < 1): leftLBL grid-0 cells 2..10 and RK(1)
-      const double UU = nu - nr.s;
-      if (-UU > nr.cut) continue;
-      if (edge) {
-        if (e == 0) { toLo = true; X = UU; }
-        else if (e == 1) { toHi = true; X = UU - 1.0; }
-        else { toLo = true; toHi = e <= 9; X = UU - (double)e; }
-      } else if (m >= 2) {
-        toLo = true;
-        X = (UU - (double)(m - 1)) - 0.5;
-      }
-    } else if (nu > nr.se) { // near-right (U < 1): rightLBL grid-0 cells 9..1, RK(1)
-      const double U = (nu - nr.s) - DELTA_WV;
-      if (U >= nr.cut) continue;
-      if (edge) {
-        if (e == 0) { toLo = toHi = true; X = U + 10.0; }
-        else if (e <= 8) { toLo = toHi = true; X = U + (double)(10 - e); }
-        else if (e == 9) { toLo = true; X = U + 1.0; }
-      } else if (m <= 9) {
-        toLo = true;
-        X = (U + (double)(10 - m)) + 0.5;
-      }
-    } else { // centre line: centerLBL grid-0 walks and RK(1)
-      const double UU = nu - nr.s;
-      if (UU >= DELTA_WV) continue;
-      const double V = DELTA_WV - UU;
-      if (edge) {
-        if (e == 0) {
-          toLo = true;
-          toHi = UU >= 2.0;
-          X = UU;
-        } else if (UU >= (double)(e + 1)) { // left walk reached cell e
-          toLo = true;
-          toHi = UU >= (double)(e + 2);
-          X = UU - (double)e;
-        } else if (V >= (double)(11 - e)) { // right walk reached cell e+1
-          toHi = e <= 9;
-          toLo = V >= (double)(12 - e);
-          X = V - (double)(10 - e);
-        }
-      } else {
-        if (UU >= (double)(m + 1)) { toLo = true; X = (UU - (double)m) + 0.5; }
-        else if (V >= (double)(12 - m)) { toLo = true; X = (V - (double)(11 - m)) + 0.5; }
-      }
-    }
-    if (!(toLo || toHi)) continue;
-    const auto f = nr.eval(q, X);
-    if (toLo) lo.add(f);
-    if (toHi) hi.add(f);
-  }
-  double vl = lo.value(), vh = hi.value();
+__device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Acc<F64> &aR, Acc<F64> (&aP)[10],
+                                           Acc<F64> (&aM)[10], Acc<F64> (&aL)[10]) {
+  const double UU = st.uu[q];
+  const int cls = q < st.c0 ? 0 : (q < st.c1 ? 1 : 2);
+  const double U = UU - DELTA_WV, V = DELTA_WV - UU;
+  const int n0 = UU >= 2.0 ? (int)floor(UU) - 1 : 0;
+  const int m0 = V >= 2.0 ? (int)floor(V) - 1 : 0;
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    vl += __shfl_down_sync(0xffffffffu, vl, off);
-    vh += __shfl_down_sync(0xffffffffu, vh, off);
-  }
-  if (lane == 0) {
-    using Real = typename Near<F64, CHI>::Real;
-    Real *o = (Real *)scr;
-    if (edge) {
-      o[e == 0 ? 0 : 21 + e - 1] = (Real)vl;            // RK(1) or L(e)
-      if (e <= 9) o[1 + e] = (Real)vh;                   // P(e+1)
+  for (int e = 0; e <= 10; ++e) {
+    bool toL = false, toP = false; // L(e) (RK(1) for e = 0) and P(e+1)
+    double X = 0.0;
+    if (cls == 0) {
+      if (e == 0) { toL = true; X = UU; }
+      else if (e == 1) { toP = true; X = UU - 1.0; }
+      else { toL = true; toP = e <= 9; X = UU - (double)e; }
+    } else if (cls == 2) {
+      if (e == 0) { toL = toP = true; X = U + 10.0; }
+      else if (e <= 8) { toL = toP = true; X = U + (double)(10 - e); }
+      else if (e == 9) { toL = true; X = U + 1.0; }
     } else {
-      o[11 + m - 1] = (Real)vl;                          // M(m)
+      if (e == 0) { toL = true; toP = n0 >= 1; X = UU; }
+      else if (e <= n0) { toL = true; toP = e + 1 <= n0; X = UU - (double)e; }
+      else if (e >= 10 - m0) { toP = e <= 9; toL = e >= 11 - m0; X = V - (double)(10 - e); }
     }
+    if (toL || toP) {
+      const auto f = st.template evalc<CHI>(q, X);
+      if (toL) {
+        if (e == 0) aR.add(f); else aL[e - 1].add(f);
+      }
+      if (toP && e <= 9) aP[e].add(f);
+    }
+  }
+#pragma unroll
+  for (int m = 1; m <= 10; ++m) {
+    bool on = false;
+    double X = 0.0;
+    if (cls == 0) { on = m >= 2; X = (UU - (double)(m - 1)) - 0.5; }
+    else if (cls == 2) { on = m <= 9; X = (U + (double)(10 - m)) + 0.5; }
+    else if (m <= n0) { on = true; X = (UU - (double)m) + 0.5; }
+    else if (m >= 11 - m0) { on = true; X = (V - (double)(11 - m)) + 0.5; }
+    if (on) aM[m - 1].add(st.template evalc<CHI>(q, X));
   }
 }
 
 // One edge site e of grid k (1..9): L(e) and P(e+1).
 template <bool F64, int CHI>
-__device__ void fine_edge_site(const Near<F64, CHI> &nr, int k, int e, int64_t &curL, int64_t &curR,
-                               void *scr) {
-  using Real = typename Near<F64, CHI>::Real;
+__device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL, int &curR, void *scr) {
+  using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
   const int ntk = nt_k(k);
   Acc<F64> aL, aP;
   aL.init();
   aP.init();
   const bool hasL = e >= 1, hasP = e <= ntk - 1;
-  // centre lines, left walk: UU in [(e+1)hk, walk_hi(e)) -> L(e); [(e+2)hk, walk_hi(e+1)) -> P(e+1)
-  {
+  { // centre lines, left walk: UU in [(e+1)hk, walk_hi(e)) -> L(e); [(e+2)hk, walk_hi(e+1)) -> P(e+1)
     const double xl0 = (double)(e + 1) * hk, xp0 = (double)(e + 2) * hk;
     const double xlh = walk_hi(e, hk), xph = walk_hi(e + 1, hk);
     const double xlo = hasL ? xl0 : xp0;
     const double xhi = hasL && hasP ? fmax(xlh, xph) : (hasL ? xlh : xph);
-    const int64_t q0 = nr.lb_uu(curL, xlo);
+    const int q0 = st.lb_uu(curL, xlo);
     curL = q0;
-    for (int64_t q = q0; q < nr.c1; ++q) {
-      const double UU = nr.uu(q);
-      if (UU >= xhi || UU >= DELTA_WV) break;
-      if (!nr.in_window(q)) continue;
+    for (int q = q0; q < st.c1; ++q) {
+      const double UU = st.uu[q];
+      if (UU >= xhi) break;
       const bool tl = hasL && UU >= xl0 && UU < xlh;
       const bool tp = hasP && UU >= xp0 && UU < xph;
       if (!(tl || tp)) continue;
-      const Real f = nr.eval(q, UU - (double)e * hk);
+      const Real f = st.template evalc<CHI>(q, UU - (double)e * hk);
       if (tl) aL.add(f);
       if (tp) aP.add(f);
     }
   }
-  // centre lines, right walk: V = 10 - UU; cell j counted r = ntk+1-j from the right
-  {
+  { // centre lines, right walk: V = 10 - UU; cell j counted r = ntk+1-j from the right
     const int rL = ntk + 1 - e, rP = ntk - e;
     const double yl0 = (double)(rL + 1) * hk, ylh = walk_hi(rL, hk);
     const double yp0 = (double)(rP + 1) * hk, yph = walk_hi(rP, hk);
     const double ylo = hasP ? yp0 : yl0;
     const double yhi = hasL && hasP ? fmax(ylh, yph) : (hasL ? ylh : yph);
-    const int64_t q0 = nr.lb_v(curR, yhi);
+    const int q0 = st.lb_v(curR, yhi);
     curR = q0;
-    for (int64_t q = q0; q < nr.c1; ++q) {
-      const double V = DELTA_WV - nr.uu(q);
+    for (int q = q0; q < st.c1; ++q) {
+      const double V = DELTA_WV - st.uu[q];
       if (V < ylo) break;
-      if (!nr.in_window(q)) continue;
       const bool tl = hasL && V >= yl0 && V < ylh;
       const bool tp = hasP && V >= yp0 && V < yph;
       if (!(tl || tp)) continue;
-      const Real f = nr.eval(q, V - (double)rP * hk);
+      const Real f = st.template evalc<CHI>(q, V - (double)rP * hk);
       if (tl) aL.add(f);
       if (tp) aP.add(f);
     }
   }
-  // near-left lines (D = -UU < 1): cells 1, 2 of grid k (leftLBL labels 20-28, 121-129)
-  if (e <= 2) {
-    const int64_t q0 = gallop_lb(nr.a, nr.c0, [&](int64_t q) { return nr.uu(q) > -hk1; });
-    for (int64_t q = q0; q < nr.c0; ++q) {
-      if (!nr.in_window(q)) continue;
-      const double UU = nr.uu(q), D = -UU;
-      if (D > nr.cut) continue;
+  if (e <= 2) { // near-left lines (D = -UU < 1): cells 1, 2 of grid k (leftLBL labels 20-28, 121-129)
+    const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
+    for (int q = q0; q < st.c0; ++q) {
+      const double UU = st.uu[q], D = -UU;
       const bool own = D >= hk; // H_k <= D < H_{k-1}: cells 1 and 2 of this grid
       double X;
       bool tl = false, tp = false;
@@ -588,18 +557,15 @@ __device__ void fine_edge_site(const Near<F64, CHI> &nr, int k, int e, int64_t &
       else if (e == 1) { tl = own; tp = true; X = UU - hk; }
       else { tl = true; X = UU - hk1; }
       if (!(tl || tp)) continue;
-      const Real f = nr.eval(q, X);
+      const Real f = st.template evalc<CHI>(q, X);
       if (tl) aL.add(f);
       if (tp) aP.add(f);
     }
   }
-  // near-right lines (U < 1): cells ntk, ntk-1 (rightLBL labels 60-69, 131-139)
-  if (e >= ntk - 2) {
-    const int64_t q1 = gallop_lb(nr.c1, nr.b, [&](int64_t q) { return (nr.uu(q) - DELTA_WV) >= hk1; });
-    for (int64_t q = nr.c1; q < q1; ++q) {
-      if (!nr.in_window(q)) continue;
-      const double U = nr.uu(q) - DELTA_WV;
-      if (U >= nr.cut) continue;
+  if (e >= ntk - 2) { // near-right lines (U < 1): cells ntk, ntk-1 (rightLBL labels 60-69, 131-139)
+    const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
+    for (int q = st.c1; q < q1; ++q) {
+      const double U = st.uu[q] - DELTA_WV;
       const bool own = U >= hk;
       double X;
       bool tl = false, tp = false;
@@ -607,7 +573,7 @@ __device__ void fine_edge_site(const Near<F64, CHI> &nr, int k, int e, int64_t &
       else if (e == ntk - 1) { tp = own; tl = true; X = U + hk; }
       else { tp = true; X = U + hk1; }
       if (!(tl || tp)) continue;
-      const Real f = nr.eval(q, X);
+      const Real f = st.template evalc<CHI>(q, X);
       if (tl) aL.add(f);
       if (tp) aP.add(f);
     }
@@ -620,9 +586,8 @@ __device__ void fine_edge_site(const Near<F64, CHI> &nr, int k, int e, int64_t &
 
 // One mid site m of grid k (1..9): M(m).
 template <bool F64, int CHI>
-__device__ void fine_mid_site(const Near<F64, CHI> &nr, int k, int m, int64_t &curL, int64_t &curR,
-                              void *scr) {
-  using Real = typename Near<F64, CHI>::Real;
+__device__ void fine_mid_site(const NearStore<F64> &st, int k, int m, int &curL, int &curR, void *scr) {
+  using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
   const double hn = h_k(k + 1); // H_{k+1}; grid 9 writes H+H, the same number
   const int ntk = nt_k(k);
@@ -630,50 +595,44 @@ __device__ void fine_mid_site(const Near<F64, CHI> &nr, int k, int m, int64_t &c
   aM.init();
   {
     const double x0 = (double)(m + 1) * hk, xh = walk_hi(m, hk);
-    const int64_t q0 = nr.lb_uu(curL, x0);
+    const int q0 = st.lb_uu(curL, x0);
     curL = q0;
-    for (int64_t q = q0; q < nr.c1; ++q) {
-      const double UU = nr.uu(q);
-      if (UU >= xh || UU >= DELTA_WV) break;
-      if (!nr.in_window(q)) continue;
-      aM.add(nr.eval(q, (UU - (double)m * hk) + hn));
+    for (int q = q0; q < st.c1; ++q) {
+      const double UU = st.uu[q];
+      if (UU >= xh) break;
+      aM.add(st.template evalc<CHI>(q, (UU - (double)m * hk) + hn));
     }
   }
   {
     const int r = ntk + 1 - m;
     const double y0 = (double)(r + 1) * hk, yh = walk_hi(r, hk);
-    const int64_t q0 = nr.lb_v(curR, yh);
+    const int q0 = st.lb_v(curR, yh);
     curR = q0;
-    for (int64_t q = q0; q < nr.c1; ++q) {
-      const double V = DELTA_WV - nr.uu(q);
+    for (int q = q0; q < st.c1; ++q) {
+      const double V = DELTA_WV - st.uu[q];
       if (V < y0) break;
-      if (!nr.in_window(q)) continue;
-      aM.add(nr.eval(q, (V - (double)r * hk) + hn));
+      aM.add(st.template evalc<CHI>(q, (V - (double)r * hk) + hn));
     }
   }
   if (m <= 2) {
-    const int64_t q0 = gallop_lb(nr.a, nr.c0, [&](int64_t q) { return nr.uu(q) > -hk1; });
-    for (int64_t q = q0; q < nr.c0; ++q) {
-      if (!nr.in_window(q)) continue;
-      const double UU = nr.uu(q), D = -UU;
-      if (D > nr.cut) continue;
+    const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
+    for (int q = q0; q < st.c0; ++q) {
+      const double UU = st.uu[q], D = -UU;
       if (m == 1) {
-        if (D >= hk) aM.add(nr.eval(q, UU - hn));
+        if (D >= hk) aM.add(st.template evalc<CHI>(q, UU - hn));
       } else {
-        aM.add(nr.eval(q, (UU - hk) - hn));
+        aM.add(st.template evalc<CHI>(q, (UU - hk) - hn));
       }
     }
   }
   if (m >= ntk - 1) {
-    const int64_t q1 = gallop_lb(nr.c1, nr.b, [&](int64_t q) { return (nr.uu(q) - DELTA_WV) >= hk1; });
-    for (int64_t q = nr.c1; q < q1; ++q) {
-      if (!nr.in_window(q)) continue;
-      const double U = nr.uu(q) - DELTA_WV;
-      if (U >= nr.cut) continue;
+    const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
+    for (int q = st.c1; q < q1; ++q) {
+      const double U = st.uu[q] - DELTA_WV;
       if (m == ntk) {
-        if (U >= hk) aM.add(nr.eval(q, U + hn));
+        if (U >= hk) aM.add(st.template evalc<CHI>(q, U + hn));
       } else {
-        aM.add(nr.eval(q, (U + hk) + hn));
+        aM.add(st.template evalc<CHI>(q, (U + hk) + hn));
       }
     }
   }
@@ -683,60 +642,47 @@ __device__ void fine_mid_site(const Near<F64, CHI> &nr, int k, int m, int64_t &c
 
 // One finest point i (2..NT): direct contributions to RK(i).
 template <bool F64, int CHI>
-__device__ void fine_point_site(const Near<F64, CHI> &nr, int i, int64_t &curL, int64_t &curR,
-                                void *scr) {
-  using Real = typename Near<F64, CHI>::Real;
+__device__ void fine_point_site(const NearStore<F64> &st, int i, int &curL, int &curR, void *scr) {
+  using Real = typename NearStore<F64>::Real;
   const double H = HSTEP, H9 = h_k(9);
   const double xi = (double)(i - 1) * H;
   Acc<F64> a;
   a.init();
-  // centre lines, left fine loop (LineGridCalc.f90:332-339):
-  // UU in [(i-1)H, (4q+8)H), q = (i-2)/4
+  // centre lines, left fine loop (LineGridCalc.f90:332-339): UU in [(i-1)H, (4q+8)H), q = (i-2)/4
   const double xh = (double)(4 * ((i - 2) / 4) + 8) * H;
-  const int64_t qa = nr.lb_uu(curL, xi);
+  const int qa = st.lb_uu(curL, xi);
   curL = qa;
-  for (int64_t q = qa; q < nr.c1; ++q) {
-    const double UU = nr.uu(q);
-    if (UU >= xh || UU >= DELTA_WV) break;
-    if (!nr.in_window(q)) continue;
-    a.add(nr.eval(q, UU - xi));
+  for (int q = qa; q < st.c1; ++q) {
+    const double UU = st.uu[q];
+    if (UU >= xh) break;
+    a.add(st.template evalc<CHI>(q, UU - xi));
   }
-  // centre lines, right fine loop (LineGridCalc.f90:485-490):
-  // UU < (i-1)H and V < H9 ((NT-i)/4 + 2)
+  // centre lines, right fine loop (LineGridCalc.f90:485-490): UU < (i-1)H and V < H9 ((NT-i)/4 + 2)
   const double yv = (double)((NT - i) / 4 + 2) * H9;
-  const int64_t qb = nr.lb_v(curR, yv);
+  const int qb = st.lb_v(curR, yv);
   curR = qb;
-  for (int64_t q = qb; q < qa; ++q) {
-    if (!nr.in_window(q)) continue;
-    a.add(nr.eval(q, nr.uu(q) - xi));
-  }
-  // near-left lines with D < H9 (leftLBL label 29)
-  if (i <= 5) {
-    const int64_t q0 = gallop_lb(nr.a, nr.c0, [&](int64_t q) { return nr.uu(q) > -H9; });
-    for (int64_t q = q0; q < nr.c0; ++q) {
-      if (!nr.in_window(q)) continue;
-      const double UU = nr.uu(q);
-      if (-UU > nr.cut) continue;
+  for (int q = qb; q < qa; ++q) a.add(st.template evalc<CHI>(q, st.uu[q] - xi));
+  if (i <= 5) { // near-left lines with D < H9 (leftLBL label 29)
+    const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -H9; });
+    for (int q = q0; q < st.c0; ++q) {
+      const double UU = st.uu[q];
       const double X = i == 2 ? UU - H : (i == 3 ? (UU - H) - H : (i == 4 ? (UU + H) - H9 : UU - H9));
-      a.add(nr.eval(q, X));
+      a.add(st.template evalc<CHI>(q, X));
     }
   }
-  // near-right lines with U < H9 (rightLBL label 69)
-  if (i >= NT - 3) {
-    const int64_t q1 = gallop_lb(nr.c1, nr.b, [&](int64_t q) { return (nr.uu(q) - DELTA_WV) >= H9; });
-    for (int64_t q = nr.c1; q < q1; ++q) {
-      if (!nr.in_window(q)) continue;
-      const double U = nr.uu(q) - DELTA_WV;
-      if (U >= nr.cut) continue;
+  if (i >= NT - 3) { // near-right lines with U < H9 (rightLBL label 69)
+    const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= H9; });
+    for (int q = st.c1; q < q1; ++q) {
+      const double U = st.uu[q] - DELTA_WV;
       const double X = i == NT ? U : (i == NT - 1 ? U + H : (i == NT - 2 ? (U + H) + H : (U + H9) - H));
-      a.add(nr.eval(q, X));
+      a.add(st.template evalc<CHI>(q, X));
     }
   }
   Real *o = (Real *)scr;
   o[SCR_RK + i - 2] = (Real)a.value();
 }
 
-// site families of phase 2: grid k edges (k=1..9), grid k mids, finest points
+// site families of the fine phase: grid k edges (k=1..9), grid k mids, finest points
 __device__ __forceinline__ void family_of(int f, int &kind, int &k, int &n) {
   if (f < 9) { kind = 0; k = f + 1; n = nt_k(k) + 1; }
   else if (f < 18) { kind = 1; k = f - 8; n = nt_k(k); }
@@ -744,58 +690,152 @@ __device__ __forceinline__ void family_of(int f, int &kind, int &k, int &n) {
 }
 
 constexpr int FINE_RUN = 8;
+constexpr int FINE_THREADS = 512;
 
-template <bool F64, int CHI>
-__global__ void __launch_bounds__(256) fine_kernel(FineParams p) {
-  using Real = typename Near<F64, CHI>::Real;
-  const int u = p.unit0 + blockIdx.x;
-  const int l = u / p.win.n_sub, sub = u - l * p.win.n_sub;
-  __shared__ int64_t sb[4];
-  Near<F64, CHI> nr;
-  nr.snu = p.snu + (size_t)l * p.n_lines;
-  nr.sidx = p.sidx + (size_t)l * p.n_lines;
-  nr.gen = p.gen + (size_t)l * p.n_lines;
-  nr.lv = p.lv[l];
-  nr.c = p.c;
-  nr.s = p.win.sub_s[sub];
-  nr.se = p.win.sub_e[sub];
-  nr.cut = p.cutoff;
-  nr.sscale = p.sscale;
-  nr.wlo = p.win.lo[sub];
-  nr.whi = p.win.hi[sub];
-  nr.shape = p.shape;
-  if (threadIdx.x < 4) {
-    // [a, c0): near-left; [c0, c1): centre; [c1, b): near-right.
-    const int64_t n = p.n_lines;
-    const double s = nr.s, se = nr.se;
-    int64_t r;
-    auto bs = [&](auto pred) {
-      int64_t lo = 0, hi = n;
-      while (lo < hi) {
-        int64_t m = (lo + hi) >> 1;
-        if (pred(m)) hi = m; else lo = m + 1;
-      }
-      return lo;
-    };
-    const double *a = nr.snu;
-    if (threadIdx.x == 0) r = bs([&](int64_t q) { return !(a[q] < s && (a[q] - s) <= -1.0); });
-    else if (threadIdx.x == 1) r = bs([&](int64_t q) { return a[q] >= s; });
-    else if (threadIdx.x == 2) r = bs([&](int64_t q) { return a[q] > se; });
-    else r = bs([&](int64_t q) { return a[q] > se && ((a[q] - s) - DELTA_WV) >= 1.0; });
-    sb[threadIdx.x] = r;
+__device__ __forceinline__ int block_excl_scan(int v, int &total) {
+  __shared__ int ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < nw ? ws[lane] : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, off);
+      if (lane >= off) w += y;
+    }
+    if (lane < nw) ws[lane] = w;
   }
   __syncthreads();
-  nr.a = sb[0];
-  nr.c0 = sb[1];
-  nr.c1 = sb[2];
-  nr.b = sb[3];
+  total = ws[nw - 1];
+  const int r = x - v + (warp > 0 ? ws[warp - 1] : 0);
+  __syncthreads();
+  return r;
+}
+
+template <bool F64, int CHI>
+__global__ void __launch_bounds__(FINE_THREADS, 1) fine_kernel(FineParams p) {
+  using Real = typename NearStore<F64>::Real;
+  extern __shared__ __align__(16) unsigned char fine_smem[];
+  const int u = p.unit0 + blockIdx.x;
+  const int l = u / p.win.n_sub, sub = u - l * p.win.n_sub;
+  const double *snu = p.snu + (size_t)l * p.n_lines;
+  const int *sidx = p.sidx + (size_t)l * p.n_lines;
+  const LineGen *gen = p.gen + (size_t)l * p.n_lines;
+  const double s = p.win.sub_s[sub], se = p.win.sub_e[sub], cut = p.cutoff;
+  const int64_t wlo = p.win.lo[sub], whi = p.win.hi[sub];
+  __shared__ int64_t sb[4];
+  __shared__ int s_counts[2];
+  if (threadIdx.x < 4) {
+    // [a, c0): near-left; [c0, c1): centre; [c1, b): near-right (sorted order)
+    const int64_t n = p.n_lines;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const int64_t m = (lo + hi) >> 1;
+      const double v = snu[m];
+      bool pr;
+      if (threadIdx.x == 0) pr = !(v < s && (v - s) <= -1.0);
+      else if (threadIdx.x == 1) pr = v >= s;
+      else if (threadIdx.x == 2) pr = v > se;
+      else pr = v > se && ((v - s) - DELTA_WV) >= 1.0;
+      if (pr) hi = m; else lo = m + 1;
+    }
+    sb[threadIdx.x] = lo;
+  }
+  if (threadIdx.x < 2) s_counts[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t a = sb[0], c0 = sb[1], c1 = sb[2], b = sb[3];
+  const int cnt = (int)(b - a);
+  // staging area: shared memory, or this block's slice of the global staging buffer
+  const int cap = cnt <= p.smem_cap ? p.smem_cap : p.gstage_cap;
+  unsigned char *base = cnt <= p.smem_cap ? fine_smem
+                                           : (unsigned char *)p.gstage + (size_t)blockIdx.x * p.gstage_bytes;
+  NearStore<F64> st;
+  st.uu = (double *)base;
+  st.qx = st.uu + cap;
+  st.vy = st.qx + cap;
+  st.lorA = (Real *)(st.vy + cap);
+  st.g2 = st.lorA + cap;
+  st.hum = st.g2 + cap;
+  st.lv = p.lv[l];
+  st.sqrt14 = p.c.sqrt14;
+  const double sscale = F64 ? 1.0 : p.sscale;
+  // compaction: lines inside the window, within the cutoff, able to contribute
+  int m_total = 0;
+  for (int64_t q0 = a; q0 < b; q0 += blockDim.x) {
+    const int64_t q = q0 + threadIdx.x;
+    int keep = 0, cls = 1;
+    double UU = 0.0;
+    int64_t li = 0;
+    if (q < b) {
+      li = sidx[q];
+      const double v = snu[q];
+      UU = v - s;
+      if (li >= wlo && li < whi) {
+        if (v < s) { cls = 0; keep = -UU <= cut; }
+        else if (v > se) { cls = 2; keep = (UU - DELTA_WV) < cut; }
+        else keep = UU < DELTA_WV;
+      }
+    }
+    int tot;
+    const int pos = m_total + block_excl_scan(keep, tot);
+    if (keep && pos < cap) {
+      st.uu[pos] = UU;
+      if (p.shape == 0) {
+        const ShapeP<Real> sp = shape_params<Real>(gen[li], p.c, sscale);
+        st.qx[pos] = sp.qx;
+        st.vy[pos] = sp.vy;
+        st.lorA[pos] = sp.lorA;
+        st.g2[pos] = sp.g2;
+        st.hum[pos] = sp.hum;
+      } else { // diagnostic shapes: F = 1 (vy < 0) or F = |X|
+        st.qx[pos] = -1.0;
+        st.vy[pos] = p.shape == 100 ? -1.0 : 1.0;
+        st.lorA[pos] = st.g2[pos] = st.hum[pos] = (Real)0;
+      }
+      if (cls == 0) atomicAdd(&s_counts[0], 1);
+      if (cls != 2) atomicAdd(&s_counts[1], 1);
+    }
+    m_total += tot;
+  }
+  __syncthreads();
+  st.m = min(m_total, cap);
+  st.c0 = s_counts[0];
+  st.c1 = s_counts[1];
   Real *scr = (Real *)p.scratch + (size_t)blockIdx.x * SCR_STRIDE;
+  if (m_total > cap) { // cannot happen when the host sized the staging area
+    if (threadIdx.x == 0) atomicMax(p.err, 14);
+    return;
+  }
 
-  // phase 1: grid-0 sites, one warp each
-  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int site = warp; site < 21; site += nwarps) fine_grid0_site<F64, CHI>(nr, site, scr);
+  // grid 0 and RK(1): one thread per near line, block reduction
+  {
+    Acc<F64> aR, aP[10], aM[10], aL[10];
+    aR.init();
+#pragma unroll
+    for (int j = 0; j < 10; ++j) { aP[j].init(); aM[j].init(); aL[j].init(); }
+    for (int q = threadIdx.x; q < st.m; q += blockDim.x) grid0_line<F64, CHI>(st, q, aR, aP, aM, aL);
+    double v[31];
+    v[0] = aR.value();
+#pragma unroll
+    for (int j = 0; j < 10; ++j) {
+      v[1 + j] = aP[j].value();
+      v[11 + j] = aM[j].value();
+      v[21 + j] = aL[j].value();
+    }
+    __shared__ double g0[31];
+    block_reduce_store<31>(v, g0);
+    __syncthreads();
+    if (threadIdx.x < 31) scr[threadIdx.x] = (Real)g0[threadIdx.x];
+  }
 
-  // phase 2: runs of FINE_RUN consecutive sites of one family per thread
+  // grids 1..9 and finest points: runs of FINE_RUN consecutive sites per thread
   int runs_total = 0;
   for (int f = 0; f < 19; ++f) {
     int kind, k, n;
@@ -803,22 +843,48 @@ __global__ void __launch_bounds__(256) fine_kernel(FineParams p) {
     runs_total += (n + FINE_RUN - 1) / FINE_RUN;
   }
   for (int r = threadIdx.x; r < runs_total; r += blockDim.x) {
-    int f = 0, base = 0, kind = 0, k = 0, n = 0;
+    int f = 0, rbase = 0, kind = 0, k = 0, n = 0;
     for (; f < 19; ++f) {
       family_of(f, kind, k, n);
       const int nr_f = (n + FINE_RUN - 1) / FINE_RUN;
-      if (r < base + nr_f) break;
-      base += nr_f;
+      if (r < rbase + nr_f) break;
+      rbase += nr_f;
     }
-    const int first = (r - base) * FINE_RUN;
+    const int first = (r - rbase) * FINE_RUN;
     const int last = min(first + FINE_RUN, n);
-    int64_t curL = nr.c0, curR = nr.c0;
+    int curL = st.c0, curR = st.c0;
     for (int t = first; t < last; ++t) {
-      if (kind == 0) fine_edge_site<F64, CHI>(nr, k, t, curL, curR, scr);
-      else if (kind == 1) fine_mid_site<F64, CHI>(nr, k, t + 1, curL, curR, scr);
-      else fine_point_site<F64, CHI>(nr, t + 2, curL, curR, scr);
+      if (kind == 0) fine_edge_site<F64, CHI>(st, k, t, curL, curR, scr);
+      else if (kind == 1) fine_mid_site<F64, CHI>(st, k, t + 1, curL, curR, scr);
+      else fine_point_site<F64, CHI>(st, t + 2, curL, curR, scr);
     }
   }
+}
+
+// Upper bound of the near-line count of every unit (lines with shifted
+// centre within 1 cm-1 of, or inside, the subinterval).
+__global__ void near_count_kernel(FineParams p, int *counts) {
+  const int ub = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ub >= p.n_units) return;
+  const int u = p.unit0 + ub;
+  const int l = u / p.win.n_sub, sub = u - l * p.win.n_sub;
+  const double *snu = p.snu + (size_t)l * p.n_lines;
+  const double s = p.win.sub_s[sub], se = p.win.sub_e[sub];
+  int64_t lo = 0, hi = p.n_lines;
+  while (lo < hi) {
+    const int64_t m = (lo + hi) >> 1;
+    const double v = snu[m];
+    if (!(v < s && (v - s) <= -1.0)) hi = m; else lo = m + 1;
+  }
+  const int64_t a = lo;
+  lo = a;
+  hi = p.n_lines;
+  while (lo < hi) {
+    const int64_t m = (lo + hi) >> 1;
+    const double v = snu[m];
+    if (v > se && ((v - s) - DELTA_WV) >= 1.0) hi = m; else lo = m + 1;
+  }
+  counts[ub] = (int)(lo - a);
 }
 
 // ----------------------------------------------------------------- cascade
@@ -1080,20 +1146,35 @@ cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t 
   return cudaGetLastError();
 }
 
+template <bool F64, int CHI>
+static cudaError_t fine_launch(const FineParams &p, cudaStream_t st) {
+  const size_t smem = fine_smem_bytes(p.smem_cap, F64);
+  cudaError_t e = cudaFuncSetAttribute(fine_kernel<F64, CHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fine_kernel<F64, CHI><<<p.n_units, FINE_THREADS, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
 template <bool F64>
-static void fine_dispatch(const FineParams &p, int chi, cudaStream_t st) {
+static cudaError_t fine_dispatch(const FineParams &p, int chi, cudaStream_t st) {
   switch (chi) {
-  case CHI_TONKOV: fine_kernel<F64, CHI_TONKOV><<<p.n_units, 256, 0, st>>>(p); break;
-  case CHI_POLLACK: fine_kernel<F64, CHI_POLLACK><<<p.n_units, 256, 0, st>>>(p); break;
-  case CHI_PERRIN: fine_kernel<F64, CHI_PERRIN><<<p.n_units, 256, 0, st>>>(p); break;
-  default: fine_kernel<F64, CHI_NONE><<<p.n_units, 256, 0, st>>>(p); break;
+  case CHI_TONKOV: return fine_launch<F64, CHI_TONKOV>(p, st);
+  case CHI_POLLACK: return fine_launch<F64, CHI_POLLACK>(p, st);
+  case CHI_PERRIN: return fine_launch<F64, CHI_PERRIN>(p, st);
+  default: return fine_launch<F64, CHI_NONE>(p, st);
   }
 }
 
+size_t fine_smem_bytes(int cap, bool f64) { return (size_t)cap * (24 + 3 * (f64 ? 8 : 4)); }
+
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st) {
   if (p.n_units == 0) return cudaSuccess;
-  if (precision == 0) fine_dispatch<true>(p, chi, st);
-  else fine_dispatch<false>(p, chi, st);
+  return precision == 0 ? fine_dispatch<true>(p, chi, st) : fine_dispatch<false>(p, chi, st);
+}
+
+cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st) {
+  if (p.n_units == 0) return cudaSuccess;
+  near_count_kernel<<<(p.n_units + 255) / 256, 256, 0, st>>>(p, counts);
   return cudaGetLastError();
 }
 

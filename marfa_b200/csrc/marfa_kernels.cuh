@@ -79,6 +79,11 @@ struct FineParams {
   int shape;
   Consts c;
   void *scratch;                 // [n_units][SCR_STRIDE] float or double
+  int smem_cap;                  // near lines staged in shared memory
+  void *gstage;                  // global staging for units above smem_cap
+  int gstage_cap;                // lines per block in gstage
+  size_t gstage_bytes;           // bytes per block in gstage
+  int *err;
 };
 
 struct CascadeParams {
@@ -113,6 +118,8 @@ cudaError_t launch_prep(const PrepParams &p, cudaStream_t st);
 cudaError_t launch_sort(const SortParams &p, cudaStream_t st);
 cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t st);
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st);
+cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st);
+size_t fine_smem_bytes(int cap, bool f64);
 cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st);
 cudaError_t launch_count(const CountParams &p, cudaStream_t st);
 
