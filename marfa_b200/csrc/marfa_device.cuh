@@ -19,7 +19,14 @@ constexpr double DELTA_WV = 10.0;
 
 __host__ __device__ constexpr int nt_k(int k) { return NT0 << k; }
 __host__ __device__ constexpr int base_k(int k) { return NT0 * ((1 << k) - 1); }
-__host__ __device__ inline double h_k(int k) { return ldexp(1.0, -k); }
+// H_k = 2^-k, built from the exponent bits (exact, no library call)
+__host__ __device__ inline double h_k(int k) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)(1023 - k) << 52);
+#else
+  return ldexp(1.0, -k);
+#endif
+}
 
 // Accumulators of one (level, subinterval) produced by the near-line kernel:
 //   [0]            RK(1)
@@ -272,10 +279,36 @@ __device__ Real voigt_eval(double Xd, const ShapeP<Real> &p, const LevelConst &l
   return dop;
 }
 
+// Regions 1-4 only (VX < 15), out of line so that kernels keep one copy of
+// the Kuntz polynomials; region 0 is evaluated inline by the callers.
+template <typename Real, int CHI>
+__device__ __noinline__ Real voigt_core(double Xd, double qx, double vy, Real lorA, Real g2, Real hum,
+                                        double pb1, double pb2, double sqrt14) {
+  ShapeP<Real> sp;
+  sp.qx = qx;
+  sp.vy = vy;
+  sp.lorA = lorA;
+  sp.g2 = g2;
+  sp.hum = hum;
+  LevelConst lv;
+  lv.perrin_b1 = pb1;
+  lv.perrin_b2 = pb2;
+  return voigt_eval<Real, CHI>(Xd, sp, lv, sqrt14);
+}
+
 template <typename Real, int CHI>
 __device__ __forceinline__ Real voigt_general(double Xd, const LineGen &g, const LevelConst &lv,
                                               const Consts &c, double sscale) {
-  return voigt_eval<Real, CHI>(Xd, shape_params<Real>(g, c, sscale), lv, c.sqrt14);
+  const ShapeP<Real> sp = shape_params<Real>(g, c, sscale);
+  const double ax = fabs(Xd);
+  if (ax * sp.qx >= 15.0) { // region 0 inline
+    const Real axr = (Real)ax;
+    const Real lor = fast_div(sp.lorA, axr * axr + sp.g2);
+    if (CHI == CHI_NONE) return lor;
+    if (sizeof(Real) == 8) return lor * (Real)chi_factor_d<CHI>(ax, lv);
+    return lor * (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
+  }
+  return voigt_core<Real, CHI>(Xd, sp.qx, sp.vy, sp.lorA, sp.g2, sp.hum, lv.perrin_b1, lv.perrin_b2, c.sqrt14);
 }
 
 } // namespace marfa

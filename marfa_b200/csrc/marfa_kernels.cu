@@ -418,26 +418,21 @@ struct NearStore {
   LevelConst lv;
   double sqrt14;
 
-  __device__ __forceinline__ Real eval(int q, double X) const {
-    ShapeP<Real> sp;
-    sp.qx = qx[q];
-    sp.vy = vy[q];
-    sp.lorA = lorA[q];
-    sp.g2 = g2[q];
-    sp.hum = hum[q];
-    return sp.qx < 0.0 ? (sp.vy < 0.0 ? (Real)1 : (Real)fabs(X)) // diagnostic shapes
-                       : voigt_eval<Real, 0>(X, sp, lv, sqrt14);
-  }
+  // F(X) of line q: region 0 (chi-corrected Lorentz) inline, regions 1-4
+  // through the out-of-line voigt_core; diagnostic shapes are marked by qx < 0.
   template <int CHI>
   __device__ __forceinline__ Real evalc(int q, double X) const {
-    ShapeP<Real> sp;
-    sp.qx = qx[q];
-    sp.vy = vy[q];
-    sp.lorA = lorA[q];
-    sp.g2 = g2[q];
-    sp.hum = hum[q];
-    if (sp.qx < 0.0) return sp.vy < 0.0 ? (Real)1 : (Real)fabs(X);
-    return voigt_eval<Real, CHI>(X, sp, lv, sqrt14);
+    const double ax = fabs(X);
+    const double qxv = qx[q];
+    if (qxv < 0.0) return vy[q] < 0.0 ? (Real)1 : (Real)ax;
+    if (ax * qxv >= 15.0) {
+      const Real axr = (Real)ax;
+      const Real lor = fast_div(lorA[q], axr * axr + g2[q]);
+      if (CHI == CHI_NONE) return lor;
+      if (sizeof(Real) == 8) return lor * (Real)chi_factor_d<CHI>(ax, lv);
+      return lor * (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
+    }
+    return voigt_core<Real, CHI>(X, qxv, vy[q], lorA[q], g2[q], hum[q], lv.perrin_b1, lv.perrin_b2, sqrt14);
   }
   // centre lines: first q with UU >= x;  first q with V = 10 - UU < y
   __device__ __forceinline__ int lb_uu(int from, double x) const {
