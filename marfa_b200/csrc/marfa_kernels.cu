@@ -495,8 +495,20 @@ __device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Acc<
 }
 
 // One edge site e of grid k (1..9): L(e) and P(e+1).
+// Sum over the lanes of a warp (lane 0 gets the total) when `coop`.
+__device__ __forceinline__ double coop_sum(double v, bool coop) {
+  if (coop) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  }
+  return v;
+}
+
+// Sites are processed either by one thread (lane 0, stride 1) or by a whole
+// warp whose lanes stride over the contributing lines (coop).
 template <bool F64, int CHI>
-__device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL, int &curR, void *scr) {
+__device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL, int &curR, void *scr,
+                               int lane, int stride) {
   using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
   const int ntk = nt_k(k);
@@ -511,9 +523,9 @@ __device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL
     const double xhi = hasL && hasP ? fmax(xlh, xph) : (hasL ? xlh : xph);
     const int q0 = st.lb_uu(curL, xlo);
     curL = q0;
-    for (int q = q0; q < st.c1; ++q) {
+    const int q1 = st.lb_uu(q0, xhi);
+    for (int q = q0 + lane; q < q1; q += stride) {
       const double UU = st.uu[q];
-      if (UU >= xhi) break;
       const bool tl = hasL && UU >= xl0 && UU < xlh;
       const bool tp = hasP && UU >= xp0 && UU < xph;
       if (!(tl || tp)) continue;
@@ -530,9 +542,9 @@ __device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL
     const double yhi = hasL && hasP ? fmax(ylh, yph) : (hasL ? ylh : yph);
     const int q0 = st.lb_v(curR, yhi);
     curR = q0;
-    for (int q = q0; q < st.c1; ++q) {
+    const int q1 = st.lb_v(q0, ylo);
+    for (int q = q0 + lane; q < q1; q += stride) {
       const double V = DELTA_WV - st.uu[q];
-      if (V < ylo) break;
       const bool tl = hasL && V >= yl0 && V < ylh;
       const bool tp = hasP && V >= yp0 && V < yph;
       if (!(tl || tp)) continue;
@@ -543,7 +555,7 @@ __device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL
   }
   if (e <= 2) { // near-left lines (D = -UU < 1): cells 1, 2 of grid k (leftLBL labels 20-28, 121-129)
     const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
-    for (int q = q0; q < st.c0; ++q) {
+    for (int q = q0 + lane; q < st.c0; q += stride) {
       const double UU = st.uu[q], D = -UU;
       const bool own = D >= hk; // H_k <= D < H_{k-1}: cells 1 and 2 of this grid
       double X;
@@ -559,7 +571,7 @@ __device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL
   }
   if (e >= ntk - 2) { // near-right lines (U < 1): cells ntk, ntk-1 (rightLBL labels 60-69, 131-139)
     const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
-    for (int q = st.c1; q < q1; ++q) {
+    for (int q = st.c1 + lane; q < q1; q += stride) {
       const double U = st.uu[q] - DELTA_WV;
       const bool own = U >= hk;
       double X;
@@ -573,15 +585,20 @@ __device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL
       if (tp) aP.add(f);
     }
   }
-  Real *o = (Real *)scr;
-  const int cb = base_k(k) - NT0;
-  if (hasL) o[SCR_FINE_L + cb + e - 1] = (Real)aL.value();
-  if (hasP) o[SCR_FINE_P + cb + e] = (Real)aP.value();
+  const bool coop = stride > 1;
+  const double vL = coop_sum(aL.value(), coop), vP = coop_sum(aP.value(), coop);
+  if (lane == 0) {
+    Real *o = (Real *)scr;
+    const int cb = base_k(k) - NT0;
+    if (hasL) o[SCR_FINE_L + cb + e - 1] = (Real)vL;
+    if (hasP) o[SCR_FINE_P + cb + e] = (Real)vP;
+  }
 }
 
 // One mid site m of grid k (1..9): M(m).
 template <bool F64, int CHI>
-__device__ void fine_mid_site(const NearStore<F64> &st, int k, int m, int &curL, int &curR, void *scr) {
+__device__ void fine_mid_site(const NearStore<F64> &st, int k, int m, int &curL, int &curR, void *scr,
+                              int lane, int stride) {
   using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
   const double hn = h_k(k + 1); // H_{k+1}; grid 9 writes H+H, the same number
@@ -592,26 +609,22 @@ __device__ void fine_mid_site(const NearStore<F64> &st, int k, int m, int &curL,
     const double x0 = (double)(m + 1) * hk, xh = walk_hi(m, hk);
     const int q0 = st.lb_uu(curL, x0);
     curL = q0;
-    for (int q = q0; q < st.c1; ++q) {
-      const double UU = st.uu[q];
-      if (UU >= xh) break;
-      aM.add(st.template evalc<CHI>(q, (UU - (double)m * hk) + hn));
-    }
+    const int q1 = st.lb_uu(q0, xh);
+    for (int q = q0 + lane; q < q1; q += stride)
+      aM.add(st.template evalc<CHI>(q, (st.uu[q] - (double)m * hk) + hn));
   }
   {
     const int r = ntk + 1 - m;
     const double y0 = (double)(r + 1) * hk, yh = walk_hi(r, hk);
     const int q0 = st.lb_v(curR, yh);
     curR = q0;
-    for (int q = q0; q < st.c1; ++q) {
-      const double V = DELTA_WV - st.uu[q];
-      if (V < y0) break;
-      aM.add(st.template evalc<CHI>(q, (V - (double)r * hk) + hn));
-    }
+    const int q1 = st.lb_v(q0, y0);
+    for (int q = q0 + lane; q < q1; q += stride)
+      aM.add(st.template evalc<CHI>(q, ((DELTA_WV - st.uu[q]) - (double)r * hk) + hn));
   }
   if (m <= 2) {
     const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
-    for (int q = q0; q < st.c0; ++q) {
+    for (int q = q0 + lane; q < st.c0; q += stride) {
       const double UU = st.uu[q], D = -UU;
       if (m == 1) {
         if (D >= hk) aM.add(st.template evalc<CHI>(q, UU - hn));
@@ -622,7 +635,7 @@ __device__ void fine_mid_site(const NearStore<F64> &st, int k, int m, int &curL,
   }
   if (m >= ntk - 1) {
     const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
-    for (int q = st.c1; q < q1; ++q) {
+    for (int q = st.c1 + lane; q < q1; q += stride) {
       const double U = st.uu[q] - DELTA_WV;
       if (m == ntk) {
         if (U >= hk) aM.add(st.template evalc<CHI>(q, U + hn));
@@ -631,8 +644,11 @@ __device__ void fine_mid_site(const NearStore<F64> &st, int k, int m, int &curL,
       }
     }
   }
-  Real *o = (Real *)scr;
-  o[SCR_FINE_M + base_k(k) - NT0 + m - 1] = (Real)aM.value();
+  const double vM = coop_sum(aM.value(), stride > 1);
+  if (lane == 0) {
+    Real *o = (Real *)scr;
+    o[SCR_FINE_M + base_k(k) - NT0 + m - 1] = (Real)vM;
+  }
 }
 
 // One finest point i (2..NT): direct contributions to RK(i).
@@ -686,6 +702,8 @@ __device__ __forceinline__ void family_of(int f, int &kind, int &k, int &n) {
 
 constexpr int FINE_RUN = 8;
 constexpr int FINE_THREADS = 512;
+constexpr int COOP_K = 5; // grids 1..COOP_K: warp per site
+__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 
 __device__ __forceinline__ int block_excl_scan(int v, int &total) {
   __shared__ int ws[32];
@@ -830,17 +848,35 @@ __global__ void __launch_bounds__(FINE_THREADS, 1) fine_kernel(FineParams p) {
     if (threadIdx.x < 31) scr[threadIdx.x] = (Real)g0[threadIdx.x];
   }
 
-  // grids 1..9 and finest points: runs of FINE_RUN consecutive sites per thread
+  // grids 1..COOP_K: one warp per site, lanes over the contributing lines
+  {
+    const int lane = threadIdx.x & 31;
+    int curL = st.c0, curR = st.c0;
+    int prev_k = -1, prev_kind = -1;
+    int site = warp_id(), total = 0;
+    for (int kk = 1; kk <= COOP_K; ++kk) total += 2 * nt_k(kk) + 1;
+    for (; site < total; site += blockDim.x >> 5) {
+      int kk = 1, rem = site;
+      while (rem >= 2 * nt_k(kk) + 1) { rem -= 2 * nt_k(kk) + 1; ++kk; }
+      const int kind = rem <= nt_k(kk) ? 0 : 1;
+      if (kk != prev_k || kind != prev_kind) { curL = st.c0; curR = st.c0; prev_k = kk; prev_kind = kind; }
+      if (kind == 0) fine_edge_site<F64, CHI>(st, kk, rem, curL, curR, scr, lane, 32);
+      else fine_mid_site<F64, CHI>(st, kk, rem - nt_k(kk), curL, curR, scr, lane, 32);
+    }
+  }
+  // grids COOP_K+1..9 and finest points: runs of FINE_RUN consecutive sites per thread
   int runs_total = 0;
   for (int f = 0; f < 19; ++f) {
     int kind, k, n;
     family_of(f, kind, k, n);
+    if (kind != 2 && k <= COOP_K) continue;
     runs_total += (n + FINE_RUN - 1) / FINE_RUN;
   }
   for (int r = threadIdx.x; r < runs_total; r += blockDim.x) {
     int f = 0, rbase = 0, kind = 0, k = 0, n = 0;
     for (; f < 19; ++f) {
       family_of(f, kind, k, n);
+      if (kind != 2 && k <= COOP_K) continue;
       const int nr_f = (n + FINE_RUN - 1) / FINE_RUN;
       if (r < rbase + nr_f) break;
       rbase += nr_f;
@@ -849,8 +885,8 @@ __global__ void __launch_bounds__(FINE_THREADS, 1) fine_kernel(FineParams p) {
     const int last = min(first + FINE_RUN, n);
     int curL = st.c0, curR = st.c0;
     for (int t = first; t < last; ++t) {
-      if (kind == 0) fine_edge_site<F64, CHI>(st, k, t, curL, curR, scr);
-      else if (kind == 1) fine_mid_site<F64, CHI>(st, k, t + 1, curL, curR, scr);
+      if (kind == 0) fine_edge_site<F64, CHI>(st, k, t, curL, curR, scr, 0, 1);
+      else if (kind == 1) fine_mid_site<F64, CHI>(st, k, t + 1, curL, curR, scr, 0, 1);
       else fine_point_site<F64, CHI>(st, t + 2, curL, curR, scr);
     }
   }
