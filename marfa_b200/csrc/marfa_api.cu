@@ -441,8 +441,9 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     CK(cudaMemcpyAsync(ncount.data(), ctx->b_near.p, (size_t)units * 4, cudaMemcpyDeviceToHost, st), "d2h near");
     CK(cudaStreamSynchronize(st), "sync near");
     const int max_near = units ? *std::max_element(ncount.begin(), ncount.end()) : 0;
-    const int smem_max = f64 ? 4096 : 5120;
-    fn.smem_cap = std::max(256, std::min(smem_max, (max_near + 255) / 256 * 256));
+    // two blocks per SM fit when each stages at most ~100 KB of lines
+    const int smem_max = f64 ? 4096 : 2816;
+    fn.smem_cap = std::max(256, std::min(smem_max, (max_near + 127) / 128 * 128));
     fn.gstage = nullptr;
     fn.gstage_cap = 0;
     fn.gstage_bytes = 0;

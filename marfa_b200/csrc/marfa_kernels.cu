@@ -449,9 +449,19 @@ __device__ __forceinline__ double walk_hi(int j, double hk) { return (double)(2 
 
 // Grid-0 and RK(1) contributions of one near line: leftLBL grid-0 cells 2..10
 // (near-left), centerLBL walks (centre), rightLBL cells 9..1 (near-right).
+// Per-lane sums of the grid-0 near part: each lane adds only the few lines
+// it owns (a handful), the block reduction then runs in double.
+template <bool F64>
+struct Lane {
+  typename std::conditional<F64, double, float>::type v;
+  __device__ __forceinline__ void init() { v = 0; }
+  __device__ __forceinline__ void add(decltype(v) x) { v += x; }
+  __device__ __forceinline__ double value() const { return (double)v; }
+};
+
 template <bool F64, int CHI>
-__device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Acc<F64> &aR, Acc<F64> (&aP)[10],
-                                           Acc<F64> (&aM)[10], Acc<F64> (&aL)[10]) {
+__device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Lane<F64> &aR, Lane<F64> (&aP)[10],
+                                           Lane<F64> (&aM)[10], Lane<F64> (&aL)[10]) {
   const double UU = st.uu[q];
   const int cls = q < st.c0 ? 0 : (q < st.c1 ? 1 : 2);
   const double U = UU - DELTA_WV, V = DELTA_WV - UU;
@@ -733,7 +743,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int &total) {
 }
 
 template <bool F64, int CHI>
-__global__ void __launch_bounds__(FINE_THREADS, 1) fine_kernel(FineParams p) {
+__global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FineParams p) {
   using Real = typename NearStore<F64>::Real;
   extern __shared__ __align__(16) unsigned char fine_smem[];
   const int u = p.unit0 + blockIdx.x;
@@ -829,7 +839,7 @@ __global__ void __launch_bounds__(FINE_THREADS, 1) fine_kernel(FineParams p) {
 
   // grid 0 and RK(1): one thread per near line, block reduction
   {
-    Acc<F64> aR, aP[10], aM[10], aL[10];
+    Lane<F64> aR, aP[10], aM[10], aL[10];
     aR.init();
 #pragma unroll
     for (int j = 0; j < 10; ++j) { aP[j].init(); aM[j].init(); aL[j].init(); }
