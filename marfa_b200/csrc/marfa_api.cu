@@ -7,6 +7,7 @@
 // Everything per line and per grid point runs on the device.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -432,6 +433,15 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.c = cst;
     fn.scratch = ctx->b_scr.p;
     fn.err = ctx->d_err;
+    fn.phase_clock = nullptr;
+    // diagnostics: MARFA_PHASE_CLOCK=<file> records clock64 marks of every
+    // fine-kernel block of the first batch (int64 [units][6]) into <file>
+    const char *clock_path = std::getenv("MARFA_PHASE_CLOCK");
+    if (clock_path && l0 == 0) {
+      CK(ensure(ctx->b_count, (size_t)units * 6 * 8), "alloc clock");
+      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * 6 * 8, st), "memset clock");
+      fn.phase_clock = (long long *)ctx->b_count.p;
+    }
     fn.unit0 = 0;
     fn.n_units = units;
     CK(ensure(ctx->b_near, (size_t)units * 4), "alloc near counts");
@@ -463,6 +473,16 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
       if (f0) cudaEventRecord(f0, st);
       CK(launch_fine(fn, run->precision, chi, st), "fine kernel");
+      if (fn.phase_clock) {
+        std::vector<long long> pcv((size_t)nu_ * 6);
+        CK(cudaMemcpyAsync(pcv.data(), fn.phase_clock, pcv.size() * 8, cudaMemcpyDeviceToHost, st), "d2h clock");
+        CK(cudaStreamSynchronize(st), "sync clock");
+        if (FILE *f = std::fopen(clock_path, "wb")) {
+          std::fwrite(pcv.data(), 8, pcv.size(), f);
+          std::fclose(f);
+        }
+        fn.phase_clock = nullptr;
+      }
       ctx->launches += 1;
       if (f1) cudaEventRecord(f1, st);
       CascadeParams cp;

@@ -408,6 +408,9 @@ struct Acc<false> {
 // reference schedule lets contribute (inside the line window, within the
 // cutoff, centre lines with UU < 10).  Held in shared memory (or, for very
 // dense line lists, in a global staging area) as structure of arrays.
+constexpr double BUCKETS_PER_CM = 256.0;
+constexpr int NBUCKET = 2560; // buckets over the 10 cm-1 subinterval
+
 template <bool F64>
 struct NearStore {
   using Real = typename std::conditional<F64, double, float>::type;
@@ -434,12 +437,25 @@ struct NearStore {
     }
     return voigt_core<Real, CHI>(X, qxv, vy[q], lorA[q], g2[q], hum[q], lv.perrin_b1, lv.perrin_b2, sqrt14);
   }
-  // centre lines: first q with UU >= x;  first q with V = 10 - UU < y
-  __device__ __forceinline__ int lb_uu(int from, double x) const {
-    return gallop_lb(from, c1, [&](int q) { return uu[q] >= x; });
+  // first[b] = first centre line with floor(UU * 2^8) >= b, b = 0 .. NBUCKET
+  const int *first;
+  // centre lines: first q with UU >= x (start from the bucket of x, exact
+  // because the bucket width is a power of two)
+  __device__ __forceinline__ int lb_uu(int, double x) const {
+    int b = (int)floor(x * BUCKETS_PER_CM);
+    b = b < 0 ? 0 : (b > NBUCKET ? NBUCKET : b);
+    int q = first[b];
+    while (q < c1 && uu[q] < x) ++q;
+    return q;
   }
-  __device__ __forceinline__ int lb_v(int from, double y) const {
-    return gallop_lb(from, c1, [&](int q) { return DELTA_WV - uu[q] < y; });
+  // centre lines: first q with V = 10 - UU < y (one bucket of margin below
+  // 10 - y covers the rounding of V)
+  __device__ __forceinline__ int lb_v(int, double y) const {
+    int b = (int)floor((DELTA_WV - y) * BUCKETS_PER_CM) - 1;
+    b = b < 0 ? 0 : (b > NBUCKET ? NBUCKET : b);
+    int q = first[b];
+    while (q < c1 && !(DELTA_WV - uu[q] < y)) ++q;
+    return q;
   }
 };
 
@@ -775,6 +791,8 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
   __syncthreads();
   const int64_t a = sb[0], c0 = sb[1], c1 = sb[2], b = sb[3];
   const int cnt = (int)(b - a);
+  long long *pc = p.phase_clock ? p.phase_clock + (size_t)blockIdx.x * 6 : nullptr;
+  if (pc && threadIdx.x == 0) { pc[0] = clock64(); pc[5] = cnt; }
   // staging area: shared memory, or this block's slice of the global staging buffer
   const int cap = cnt <= p.smem_cap ? p.smem_cap : p.gstage_cap;
   unsigned char *base = cnt <= p.smem_cap ? fine_smem
@@ -836,7 +854,18 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
     if (threadIdx.x == 0) atomicMax(p.err, 14);
     return;
   }
+  // bucket table of the centre lines: bucket b's entry is the first line
+  // whose bucket is >= b; written by the line that opens the bucket range
+  __shared__ int s_first[NBUCKET + 1];
+  for (int q = st.c0 + threadIdx.x; q <= st.c1; q += blockDim.x) {
+    const int bq = q < st.c1 ? min((int)floor(st.uu[q] * BUCKETS_PER_CM), NBUCKET) : NBUCKET + 1;
+    const int bp = q > st.c0 ? min((int)floor(st.uu[q - 1] * BUCKETS_PER_CM), NBUCKET) : -1;
+    for (int bb = bp + 1; bb <= min(bq, NBUCKET); ++bb) s_first[bb] = q;
+  }
+  __syncthreads();
+  st.first = s_first;
 
+  if (pc && threadIdx.x == 0) pc[1] = clock64();
   // grid 0 and RK(1): one thread per near line, block reduction
   {
     Lane<F64> aR, aP[10], aM[10], aL[10];
@@ -858,6 +887,8 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
     if (threadIdx.x < 31) scr[threadIdx.x] = (Real)g0[threadIdx.x];
   }
 
+  __syncthreads();
+  if (pc && threadIdx.x == 0) pc[2] = clock64();
   // grids 1..COOP_K: one warp per site, lanes over the contributing lines
   {
     const int lane = threadIdx.x & 31;
@@ -873,6 +904,10 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
       if (kind == 0) fine_edge_site<F64, CHI>(st, kk, rem, curL, curR, scr, lane, 32);
       else fine_mid_site<F64, CHI>(st, kk, rem - nt_k(kk), curL, curR, scr, lane, 32);
     }
+  }
+  if (pc) {
+    __syncthreads();
+    if (threadIdx.x == 0) pc[3] = clock64();
   }
   // grids COOP_K+1..9 and finest points: runs of FINE_RUN consecutive sites per thread
   int runs_total = 0;
@@ -899,6 +934,10 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
       else if (kind == 1) fine_mid_site<F64, CHI>(st, k, t + 1, curL, curR, scr, 0, 1);
       else fine_point_site<F64, CHI>(st, t + 2, curL, curR, scr);
     }
+  }
+  if (pc) {
+    __syncthreads();
+    if (threadIdx.x == 0) pc[4] = clock64();
   }
 }
 
