@@ -1,0 +1,339 @@
+"""Benchmark of the B200 line-by-line core on the Venus-like PT-table workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one step): the 40-level Venus-like CO2 PT-table set -- 200,000
+seeded synthetic lines over 4000-5000 cm-1, P log-spaced 92 -> 1e-4 atm,
+T 735 -> 170 K, 96.5% CO2 by the ideal-gas law, cutoff 125 cm-1, tonkov
+chi-factor, VAC target: 40 levels x 100 subintervals x 20,481 points.
+Metric: line-grid evaluations per second (one evaluation = one line-shape
+call of the reference's multigrid schedule, counted exactly by the library),
+for the FP32-compensated form; the FP64 drop-in, the FP32c/FP64 ratio and the
+FP32c error against the FP64 result are reported beside it.
+
+Under torchrun every rank computes its own copy of the PT-table set (levels
+are independent; no collective on the data path): weak scaling, the value is
+the evaluations of all ranks over the slowest rank's time.
+
+--impl reference times the CPU restatement of the reference's own algorithm
+(oracle/, Fortran type map, all host threads) on a bounded sample of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "line-grid evals/s & s per 40-level PT set: FP32c vs FP64 GPU at <=1e-5 rel err"
+UNIT = "line-grid evals/s"
+WORKLOAD = "venus-co2-200k-lines-40-levels-4000-5000cm-1-cutoff125-tonkov-VAC"
+FLOP_PER_EVAL = 12  # chi-corrected Lorentz evaluation + accumulation, FMA = 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from marfa_b200 import synth
+    return synth.config(1)
+
+
+def tips_table():
+    from marfa_b200 import data_path
+    from marfa_b200.io import read_tips
+    return read_tips(data_path("TIPS_subset.dat"))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- CPU legs
+def cpu_baseline_sample(w, tips, levels, nthreads):
+    """Oracle (Fortran type map) on `levels` of the workload; returns
+    (evals, seconds)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from marfa_b200.io import species_code
+    p = w.profiles[0]
+    o = O.Oracle(w.lines, tips, p.pressure[levels], p.temperature[levels], p.density[levels],
+                 w.start_wv, w.end_wv, w.cutoff, target=w.target, chi=w.chi,
+                 mol_code=species_code(w.molecule), precision=O.MIXED, nthreads=nthreads)
+    t0 = time.perf_counter()
+    _, _, ev = o.run(want64=False)
+    dt = time.perf_counter() - t0
+    return int(ev.sum()), dt
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    w = workload()
+    tips = tips_table()
+    cores = os.cpu_count() or 1
+    # each step: one level per host thread (bounded sample of the 40 levels)
+    n = max(1, min(cores, 40))
+    levels = list(np.linspace(0, 39, n).round().astype(int))
+    if args.warmup > 0:  # one level, to page in the oracle and the line list
+        cpu_baseline_sample(w, tips, levels[:1], 1)
+    tot_ev, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        ev, dt = cpu_baseline_sample(w, tips, levels, cores)
+        tot_ev += ev
+        tot_t += dt
+    v = tot_ev / tot_t
+    sample = f"{n} of 40 levels x 100 subintervals per step, {cores} threads, CPU restatement (Fortran type map)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "sample_levels": n},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# --------------------------------------------------------------- GPU leg
+def timed_steps(ctx, run, p, out, stream, steps, warmup):
+    import torch
+    L = len(p.pressure)
+    for _ in range(warmup):
+        ctx.compute_device(run, [L], p.pressure, p.temperature, p.density, out.data_ptr(),
+                           stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    for _ in range(steps):
+        ctx.compute_device(run, [L], p.pressure, p.temperature, p.density, out.data_ptr(),
+                           stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    tm = ctx.timings()
+    launches = int(tm["launches"]) * steps
+    return ms, tm, launches
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    from marfa_b200 import build as B
+    from marfa_b200.api import Context, Run
+    from marfa_b200 import _lib
+    B.build()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    w = workload()
+    tips = tips_table()
+    p = w.profiles[0]
+    L = len(p.pressure)
+    ctx = Context(w.lines, tips, device=local_rank)
+    run32 = Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule, chi=w.chi,
+                precision="fp32c")
+    run64 = Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule, chi=w.chi,
+                precision="fp64")
+    ev, evf = ctx.eval_count(run32, p.pressure, p.temperature, p.density, far=True)
+    evals = int(ev.sum())
+    far_evals = int(evf.sum())
+    out32 = torch.empty((L, run32.n_sub, 20481), dtype=torch.float32, device="cuda")
+    out64 = torch.empty_like(out32)
+    stream = torch.cuda.Stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # FP32-compensated form (the headline), clocks sampled during the timed region
+    barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms32, tm32, launches = timed_steps(ctx, run32, p, out32, stream, args.steps, args.warmup)
+    clk = clocks.stop()
+    barrier()
+    # FP64 drop-in
+    ms64, tm64, _ = timed_steps(ctx, run64, p, out64, stream, max(2, args.steps // 2), 1)
+    barrier()
+    ms_max = ms32
+    if dist is not None:
+        t = torch.tensor([ms32, ms64], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max, ms64 = float(t[0]), float(t[1])
+    value = world * evals / (ms_max * 1e-3)
+    value64 = world * evals / (ms64 * 1e-3)
+
+    # accuracy of the FP32c records against the FP64 drop-in (same workload)
+    a = out32.double()
+    b = out64.double()
+    mask = b > 1e-6 * b.max()
+    rel = ((a - b).abs()[mask] / b[mask])
+    max_rel = float(rel.max())
+    p9999 = float(torch.quantile(rel[:: max(1, rel.numel() // 4_000_000)], 0.9999))
+    del a, b, rel, mask
+
+    # end to end: host profile in, host (pinned) records out, through the C ABI
+    host_out = torch.empty((L, run32.n_sub, 20481), dtype=torch.float32, pin_memory=True)
+    ctx.compute(run32, p.pressure, p.temperature, p.density, out=host_out)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = max(2, args.steps // 2)
+    for _ in range(e2e_steps):
+        ctx.compute(run32, p.pressure, p.temperature, p.density, out=host_out)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    h2d = 3 * L * 8
+    d2h = host_out.numel() * 4
+
+    # roofline of the dominant kernel family (measured FMA peak of this GPU)
+    fp32_peak = np.zeros(1)
+    fp64_peak = np.zeros(1)
+    lib = _lib.load()
+    lib.marfa_measure_fma_peak(local_rank, fp32_peak.ctypes.data, fp64_peak.ctypes.data)
+    fams = {k: tm32[k] for k in ("prep", "sort", "far", "fine", "cascade")}
+    dom = max(fams, key=fams.get)
+    fam_evals = {"far": far_evals, "fine": evals - far_evals}
+    roof = None
+    if dom in fam_evals:
+        achieved = FLOP_PER_EVAL * fam_evals[dom] / (tm32[dom] * 1e-3) / 1e12
+        peak = fp32_peak[0] / 1e12
+        roof = {"kernel": f"{dom}_kernel (fp32c)", "bound": "fp32", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "FFMA throughput measured by bench.py on this GPU"}
+    far_roof = FLOP_PER_EVAL * far_evals / (tm32["far"] * 1e-3) / 1e12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        levels = [0, 13, 26, 39]
+        cev, cdt = cpu_baseline_sample(w, tips, levels, 1)
+        cpu = {"value": cev / cdt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "levels 1, 14, 27, 40 of 40 x 100 subintervals, 1 thread, CPU "
+                         "restatement of the reference (Fortran type map), "
+                         f"{cev} evaluations in {cdt:.1f} s"}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (compensated) + fp64 offsets",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lines": int(len(w.lines) - 1), "levels": L,
+                       "subintervals": run32.n_sub, "cutoff_cm-1": w.cutoff, "chi": w.chi,
+                       "target": w.target, "l2": "inputs larger than L2 (576 MB line state, "
+                       "328 MB records per step)", "parallelism": f"replicas x{world}"},
+            "s_per_pt_set": ms_max * 1e-3,
+            "evals_per_step": evals,
+            "fp64_value": value64, "fp64_ms_per_step": ms64,
+            "fp32c_over_fp64": ms64 / ms_max,
+            "max_rel_err_fp32c_vs_fp64": max_rel, "p9999_rel_err_fp32c_vs_fp64": p9999,
+            "kernel_ms": {k: round(v, 4) for k, v in fams.items()},
+            "kernel_ms_fp64": {k: round(tm64[k], 4) for k in fams},
+            "roofline": roof,
+            "far_kernel_tflops": far_roof,
+            "fma_peak_tflops": {"fp32": fp32_peak[0] / 1e12, "fp64": fp64_peak[0] / 1e12},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * evals / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }))
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_b200(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

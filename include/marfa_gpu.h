@@ -163,6 +163,11 @@ int marfa_debug_accumulators(marfa_ctx *ctx, const marfa_run *run, const double 
  * kernel launches and the number of far-kernel launches. */
 int marfa_last_timings(marfa_ctx *ctx, double *times);
 
+/* Measured FP32 and FP64 FMA throughput of `device` (FLOP/s, FMA = 2):
+ * the denominators of the shape kernels' roofline, which run on the
+ * non-tensor FP32 / FP64 pipes. */
+int marfa_measure_fma_peak(int device, double *fp32_flops, double *fp64_flops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,7 +21,7 @@ EXPORTS = (
     "marfa_ctx_create", "marfa_ctx_destroy", "marfa_last_error", "marfa_num_subintervals",
     "marfa_record_number", "marfa_compute", "marfa_compute_batched", "marfa_compute_device",
     "marfa_synchronize", "marfa_eval_count", "marfa_debug_accumulators", "marfa_last_timings",
-    "marfa_plan_windows",
+    "marfa_plan_windows", "marfa_measure_fma_peak",
 )
 
 
@@ -71,6 +71,7 @@ def load():
         "marfa_debug_accumulators": (I, [P, ctypes.POINTER(MarfaRun), P, P, P, I, I, I, P]),
         "marfa_last_timings": (I, [P, P]),
         "marfa_plan_windows": (I, [P, I64, D, D, D, P, P]),
+        "marfa_measure_fma_peak": (I, [I, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -826,6 +826,14 @@ int marfa_debug_accumulators(marfa_ctx *ctx, const marfa_run *run, const double 
   }
 }
 
+int marfa_measure_fma_peak(int device, double *fp32_flops, double *fp64_flops) {
+  if (!fp32_flops || !fp64_flops) return MARFA_E_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return MARFA_E_NODEVICE;
+  if (fma_peak(false, fp32_flops) != cudaSuccess) return MARFA_E_CUDA;
+  if (fma_peak(true, fp64_flops) != cudaSuccess) return MARFA_E_CUDA;
+  return MARFA_OK;
+}
+
 int marfa_last_timings(marfa_ctx *ctx, double *times) {
   if (!ctx || !times) return MARFA_E_ARG;
   for (int i = 0; i < 8; ++i) times[i] = 0.0;

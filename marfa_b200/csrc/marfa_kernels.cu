@@ -1187,6 +1187,54 @@ __global__ void __launch_bounds__(256) count_kernel(CountParams p) {
   }
 }
 
+// ------------------------------------------------------- pipe peak probes
+// Chains of independent FMAs: the measured FP32 / FP64 FMA throughput of this
+// GPU, used as the roofline denominator of the (non-tensor) shape kernels.
+template <typename T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T *sink, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x[j] = (T)(threadIdx.x + j);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = x[j] * a + b;
+  }
+  T s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += x[j];
+  if (s == (T)-1.2345) sink[threadIdx.x] = s; // keeps the chains alive
+}
+
+cudaError_t fma_peak(bool f64, double *flops_per_s) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  void *sink = nullptr;
+  cudaError_t e = cudaMalloc(&sink, 4096);
+  if (e != cudaSuccess) return e;
+  const int blocks = nsm * 8, iters = f64 ? 4096 : 16384;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(e0);
+    if (f64) fma_peak_kernel<double><<<blocks, 256>>>((double *)sink, iters, 0.999999, 1e-7);
+    else fma_peak_kernel<float><<<blocks, 256>>>((float *)sink, iters, 0.9999f, 1e-7f);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0) best = ms < best ? ms : best;
+  }
+  e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  *flops_per_s = 2.0 * 8.0 * (double)iters * blocks * 256 / (best * 1e-3);
+  return e;
+}
+
 // --------------------------------------------------------------- launchers
 static bool wiso_loaded = false;
 

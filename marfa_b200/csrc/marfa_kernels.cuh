@@ -121,6 +121,7 @@ cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t 
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st);
 cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st);
 size_t fine_smem_bytes(int cap, bool f64);
+cudaError_t fma_peak(bool f64, double *flops_per_s);
 cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st);
 cudaError_t launch_count(const CountParams &p, cudaStream_t st);
 
