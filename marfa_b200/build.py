@@ -19,6 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libmarfa_gpu.so"
+CLI = PKG / "marfa"
 SOURCES = ["marfa_kernels.cu", "marfa_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -48,7 +49,10 @@ def stale() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
+    if not CLI.exists():
+        return True
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + \
+        list(CSRC.glob("*.cpp")) + \
         list((ROOT / "include").glob("*.h")) + [Path(__file__)]
     return any(d.stat().st_mtime > t for d in deps)
 
@@ -65,6 +69,12 @@ def build(force: bool = False, extra=()) -> Path:
     if r.returncode:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    # the `marfa` command (host driver over the C ABI)
+    cmd = [nvcc(), "-O2", "-std=c++17", "-I", str(ROOT / "include"), str(CSRC / "marfa_cli.cpp"),
+           "-o", str(CLI), "-L", str(PKG), "-lmarfa_gpu", "-Xlinker", "-rpath=$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode:
+        raise RuntimeError(f"marfa command build failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

@@ -228,6 +228,9 @@ int build_levels(marfa_ctx *ctx, int n, const double *P, const double *T, const 
     v.T = T[l];
     v.density = dens[l];
     v.pself = dens[l] * 10.0 * c.bolsi * T[l] / c.stdp; // main.f90:92
+    if (v.pself > P[l] * (1.0 + 1e-6))
+      return set_err(ctx, 7, "level %d: partial pressure %.6g atm from the density exceeds the total "
+                             "pressure %.6g atm", l + 1, v.pself, P[l]);
     v.perrin_b1 = 0.0888 - 0.16 * std::exp(-(0.00410 * T[l]));
     v.perrin_b2 = 0.0526 * std::exp(-(0.00152 * T[l]));
   }

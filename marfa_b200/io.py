@@ -95,13 +95,13 @@ def read_profile(path):
 
 
 def write_profile(path, title, height, P, T, n) -> None:
-    """Write a profile so that every value is the exact decimal of a float32
-    (the reference parses them into default reals)."""
+    """Write a profile whose values are float32 numbers printed exactly (the
+    reference parses them into default reals; a double parse of the text
+    gives the same value)."""
     with open(path, "w") as f:
         f.write(f"{title[:20]}\n{len(P)}\n")
         for h, p, t, d in zip(height, P, T, n):
-            f.write(" ".join(f"{np.float32(v)!r}".replace("np.float32(", "").rstrip(")")
-                             for v in (h, p, t, d)) + "\n")
+            f.write(" ".join(repr(float(np.float32(v))) for v in (h, p, t, d)) + "\n")
 
 
 def read_tips(path):
