@@ -199,3 +199,14 @@ def test_cascade_is_exact_at_grid0_lattice_points(tips):
     for j in range(11):
         v, _ = o.shape_value(0, 0, 4050.0 + j - 4053.3)
         assert abs(rec[2048 * j] - v) <= 1e-12 * v
+
+
+def test_cascade_restatement_used_by_the_fp32c_check(cfg0, tips):
+    """The vectorised cascade of tests/fp32c_check.py reproduces the oracle's
+    records from the oracle's raw accumulators."""
+    from fp32c_check import tainted_points
+    o = O.from_workload(cfg0, precision=O.FP64, tips=tips)
+    rec = o.run()[1][0]
+    for isub in (0, 5, 9):
+        _, rk = tainted_points(o.accumulators(0, isub), want_record=True)
+        assert np.max(np.abs(rk - rec[isub]) / rec[isub]) < 1e-13
