@@ -133,9 +133,9 @@ def test_error_statuses(gpu, tips):
         with pytest.raises(MarfaError) as e:
             Run(4000, 4100, 25, molecule="XE").c()
         assert e.value.code == 8
-        bad = Run(w.start_wv, 4200.0, w.cutoff, molecule="CO2")   # windows run off the list
+    with Context(w.lines[:-1], tips) as ctx:                   # no line beyond the last window
         with pytest.raises(MarfaError) as e:
-            ctx.compute(bad, p.pressure, p.temperature, p.density)
+            ctx.compute(run, p.pressure, p.temperature, p.density)
         assert e.value.code == 9
     unsorted = w.lines.copy()
     unsorted["nu"][[3, 4]] = unsorted["nu"][[4, 3]]
