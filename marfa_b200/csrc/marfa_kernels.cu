@@ -1236,13 +1236,18 @@ cudaError_t fma_peak(bool f64, double *flops_per_s) {
 }
 
 // --------------------------------------------------------------- launchers
-static bool wiso_loaded = false;
+// the WISO table lives in constant memory, one copy per device
+static bool wiso_loaded[256] = {};
 
 cudaError_t launch_prep(const PrepParams &p, cudaStream_t st) {
-  if (!wiso_loaded) {
-    cudaError_t e = cudaMemcpyToSymbol(c_wiso, MARFA_WISO_D, sizeof(MARFA_WISO_D));
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+  if (!wiso_loaded[dev]) {
+    e = cudaMemcpyToSymbol(c_wiso, MARFA_WISO_D, sizeof(MARFA_WISO_D));
     if (e != cudaSuccess) return e;
-    wiso_loaded = true;
+    wiso_loaded[dev] = true;
   }
   dim3 grid((unsigned)((p.lines.n + 255) / 256), (unsigned)p.n_levels);
   prep_kernel<<<grid, 256, 0, st>>>(p);
