@@ -37,6 +37,8 @@ extern "C" {
 #define MARFA_E_TEMPERATURE 11  /* level temperature outside the TIPS table          */
 #define MARFA_E_UNSORTED 12     /* line list not sorted by wavenumber                */
 #define MARFA_E_ISOTOPE 13      /* jointMolIso/100 outside the WISO/TIPS tables      */
+#define MARFA_E_CAPACITY 15     /* input larger than marfa_compute_record_static's   */
+                                /* fixed storage                                     */
 #define MARFA_E_CUDA 100        /* CUDA runtime error (see marfa_last_error)         */
 #define MARFA_E_NOMEM 101       /* device allocation failed                          */
 #define MARFA_E_NODEVICE 110    /* no CUDA device                                    */
@@ -162,6 +164,35 @@ int marfa_debug_accumulators(marfa_ctx *ctx, const marfa_run *run, const double 
  * kernel family (prep, sort, far, fine, cascade), the total, the number of
  * kernel launches and the number of far-kernel launches. */
 int marfa_last_timings(marfa_ctx *ctx, double *times);
+
+/* One PT record (one level, one subinterval) computed without allocating any
+ * memory.  This entry point has no counterpart in the reference, which
+ * computes whole profiles; it exists for callers that cannot call cudaMalloc,
+ * for example applications whose device memory is owned by a pool allocator
+ * that reserves the GPU at start-up, or loops that cannot afford
+ * cudaMalloc's implicit device synchronisation.  All device working storage
+ * is one static array of MARFA_STATIC_SCRATCH_BYTES inside the library, held
+ * by every GPU that loads the library until the process exits.
+ *   lines, n_lines: all line records (sorted, ending beyond the last window);
+ *   only the window of subinterval `isub` (at most
+ *   MARFA_STATIC_MAX_WINDOW_LINES lines, of which at most
+ *   MARFA_STATIC_MAX_NEAR_LINES within 1 cm-1 of the subinterval when they do
+ *   not fit on chip) is copied to the device; larger inputs return
+ *   MARFA_E_CAPACITY.
+ *   tips: [n_iso][n_temp] (at most 131,072 values); pressure, temperature,
+ *   density: the level; record: 20481 floats, host or device memory.
+ *   stream: cudaStream_t or NULL; the call waits for its work to finish.
+ *   msg (optional): receives a text description of a failure.
+ * The first call on each device looks up the array's device address and
+ * should come before any stream capture.  Every call on a device reuses the
+ * same array: calls that overlap on the GPU race. */
+#define MARFA_STATIC_MAX_WINDOW_LINES 65536
+#define MARFA_STATIC_MAX_NEAR_LINES 8192
+#define MARFA_STATIC_SCRATCH_BYTES (11u * 1024u * 1024u)
+int marfa_compute_record_static(const marfa_line_record *lines, int64_t n_lines, const double *tips,
+                                int n_iso, int n_temp, const marfa_run *run, double pressure,
+                                double temperature, double density, int isub, float *record,
+                                void *stream, char *msg, size_t msg_len);
 
 /* Measured FP32 and FP64 FMA throughput of `device` (FLOP/s, FMA = 2):
  * the denominators of the shape kernels' roofline, which run on the

@@ -21,7 +21,7 @@ EXPORTS = (
     "marfa_ctx_create", "marfa_ctx_destroy", "marfa_last_error", "marfa_num_subintervals",
     "marfa_record_number", "marfa_compute", "marfa_compute_batched", "marfa_compute_device",
     "marfa_synchronize", "marfa_eval_count", "marfa_debug_accumulators", "marfa_last_timings",
-    "marfa_plan_windows", "marfa_measure_fma_peak",
+    "marfa_plan_windows", "marfa_measure_fma_peak", "marfa_compute_record_static",
 )
 
 
@@ -72,6 +72,8 @@ def load():
         "marfa_last_timings": (I, [P, P]),
         "marfa_plan_windows": (I, [P, I64, D, D, D, P, P]),
         "marfa_measure_fma_peak": (I, [I, P, P]),
+        "marfa_compute_record_static": (I, [P, I64, P, I, I, ctypes.POINTER(MarfaRun), D, D, D, I, P,
+                                            P, ctypes.c_char_p, ctypes.c_size_t]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
