@@ -438,11 +438,11 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.err = ctx->d_err;
     fn.phase_clock = nullptr;
     // diagnostics: MARFA_PHASE_CLOCK=<file> records clock64 marks of every
-    // fine-kernel block of the first batch (int64 [units][6]) into <file>
+    // fine-kernel block of the first batch (int64 [units][10]: phase marks, near count, per-family run cycles) into <file>
     const char *clock_path = std::getenv("MARFA_PHASE_CLOCK");
     if (clock_path && l0 == 0) {
-      CK(ensure(ctx->b_count, (size_t)units * 6 * 8), "alloc clock");
-      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * 6 * 8, st), "memset clock");
+      CK(ensure(ctx->b_count, (size_t)units * 10 * 8), "alloc clock");
+      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * 10 * 8, st), "memset clock");
       fn.phase_clock = (long long *)ctx->b_count.p;
     }
     fn.unit0 = 0;
@@ -477,7 +477,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       if (f0) cudaEventRecord(f0, st);
       CK(launch_fine(fn, run->precision, chi, st), "fine kernel");
       if (fn.phase_clock) {
-        std::vector<long long> pcv((size_t)nu_ * 6);
+        std::vector<long long> pcv((size_t)nu_ * 10);
         CK(cudaMemcpyAsync(pcv.data(), fn.phase_clock, pcv.size() * 8, cudaMemcpyDeviceToHost, st), "d2h clock");
         CK(cudaStreamSynchronize(st), "sync clock");
         if (FILE *f = std::fopen(clock_path, "wb")) {

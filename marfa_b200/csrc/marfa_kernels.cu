@@ -791,7 +791,9 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
   __syncthreads();
   const int64_t a = sb[0], c0 = sb[1], c1 = sb[2], b = sb[3];
   const int cnt = (int)(b - a);
-  long long *pc = p.phase_clock ? p.phase_clock + (size_t)blockIdx.x * 6 : nullptr;
+  long long *pc = p.phase_clock ? p.phase_clock + (size_t)blockIdx.x * 10 : nullptr;
+  __shared__ long long s_fam[3];
+  if (threadIdx.x < 3) s_fam[threadIdx.x] = 0;
   if (pc && threadIdx.x == 0) { pc[0] = clock64(); pc[5] = cnt; }
   // staging area: shared memory, or this block's slice of the global staging buffer
   const int cap = cnt <= p.smem_cap ? p.smem_cap : p.gstage_cap;
@@ -929,15 +931,22 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
     const int first = (r - rbase) * FINE_RUN;
     const int last = min(first + FINE_RUN, n);
     int curL = st.c0, curR = st.c0;
+    const long long tr0 = pc ? clock64() : 0;
     for (int t = first; t < last; ++t) {
       if (kind == 0) fine_edge_site<F64, CHI>(st, k, t, curL, curR, scr, 0, 1);
       else if (kind == 1) fine_mid_site<F64, CHI>(st, k, t + 1, curL, curR, scr, 0, 1);
       else fine_point_site<F64, CHI>(st, t + 2, curL, curR, scr);
     }
+    if (pc) atomicAdd((unsigned long long *)&s_fam[kind], (unsigned long long)(clock64() - tr0));
   }
   if (pc) {
     __syncthreads();
-    if (threadIdx.x == 0) pc[4] = clock64();
+    if (threadIdx.x == 0) {
+      pc[4] = clock64();
+      pc[6] = s_fam[0];
+      pc[7] = s_fam[1];
+      pc[8] = s_fam[2];
+    }
   }
 }
 

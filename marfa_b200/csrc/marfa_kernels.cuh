@@ -84,7 +84,7 @@ struct FineParams {
   int gstage_cap;                // lines per block in gstage
   size_t gstage_bytes;           // bytes per block in gstage
   int *err;
-  long long *phase_clock;        // optional [n_units][6] clock64 marks (diagnostics)
+  long long *phase_clock;        // optional [n_units][10] clock64 marks (diagnostics)
 };
 
 struct CascadeParams {
