@@ -144,6 +144,27 @@ int marfa_compute_device(marfa_ctx *ctx, const marfa_run *run, int n_profiles,
                          float *device_out, void *stream);
 int marfa_synchronize(marfa_ctx *ctx);
 
+/* Replaces the reference intensities S and air-broadening coefficients
+ * gamma_air of every line by double values (either pointer may be NULL: back
+ * to the database record's float value).  The reference reads both from the
+ * line record (LBL.f90:43-44); this is the parameter update of a retrieval
+ * that differentiates with respect to them (marfa_vjp). */
+int marfa_ctx_set_line_params(marfa_ctx *ctx, const double *S, const double *gamma_air);
+
+/* Vector-Jacobian product of the records.  For the cotangent
+ * cotangent[n_levels][n_sub][MARFA_NT] (host, double) of the FP64 records
+ * (out64 of marfa_compute) it returns dL/dT and dL/dP per level and dL/dS and
+ * dL/dgamma_air per line (host arrays [n_levels] and [n_lines]) of
+ * L = sum cotangent * record, holding the placement of each line, the
+ * Humlicek region choices and the cascade clamp decisions fixed.  The line
+ * shape is recomputed, nothing of the forward pass is stored.  Voigt shape
+ * only; run->precision is ignored (FP64).  No reference counterpart: the
+ * reference has no derivatives. */
+int marfa_vjp(marfa_ctx *ctx, const marfa_run *run, const double *pressure,
+              const double *temperature, const double *density, int n_levels,
+              const double *cotangent, double *d_temperature, double *d_pressure,
+              double *d_S, double *d_gamma_air);
+
 /* Number of line-shape evaluations the reference schedule performs for this
  * workload (FSHAPE calls of LineGridCalc.f90), per level; far_per_level
  * (optional) receives the part made by lines at least 1 cm-1 outside their

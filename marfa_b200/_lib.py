@@ -22,6 +22,7 @@ EXPORTS = (
     "marfa_record_number", "marfa_compute", "marfa_compute_batched", "marfa_compute_device",
     "marfa_synchronize", "marfa_eval_count", "marfa_debug_accumulators", "marfa_last_timings",
     "marfa_plan_windows", "marfa_measure_fma_peak", "marfa_compute_record_static",
+    "marfa_ctx_set_line_params", "marfa_vjp",
 )
 
 
@@ -74,6 +75,8 @@ def load():
         "marfa_measure_fma_peak": (I, [I, P, P]),
         "marfa_compute_record_static": (I, [P, I64, P, I, I, ctypes.POINTER(MarfaRun), D, D, D, I, P,
                                             P, ctypes.c_char_p, ctypes.c_size_t]),
+        "marfa_ctx_set_line_params": (I, [P, P, P]),
+        "marfa_vjp": (I, [P, ctypes.POINTER(MarfaRun), P, P, P, I, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -146,6 +146,40 @@ class Context:
     def synchronize(self):
         self._check(self._lib.marfa_synchronize(self._h))
 
+    @property
+    def n_lines(self) -> int:
+        return len(self._lines)
+
+    def set_line_params(self, S=None, gamma_air=None):
+        """Double-precision reference intensities and air-broadening
+        coefficients for every line (None: the database record's value)."""
+        self._S64 = None if S is None else _f64(S)
+        self._g64 = None if gamma_air is None else _f64(gamma_air)
+        for a in (self._S64, self._g64):
+            if a is not None and a.shape != (self.n_lines,):
+                raise ValueError(f"expected {self.n_lines} values, got {a.shape}")
+        self._check(self._lib.marfa_ctx_set_line_params(
+            self._h, ctypes.c_void_p(0 if self._S64 is None else self._S64.ctypes.data),
+            ctypes.c_void_p(0 if self._g64 is None else self._g64.ctypes.data)))
+
+    def vjp(self, run: Run, pressure, temperature, density, cotangent) -> dict:
+        """Vector-Jacobian product of the FP64 records for `cotangent`
+        [n_levels, n_sub, 20481]: dict of dT, dP [n_levels] and dS,
+        dgamma_air [n_lines] (float64)."""
+        P, T, n = _f64(pressure), _f64(temperature), _f64(density)
+        cot = _f64(cotangent)
+        if cot.shape != (len(P), run.n_sub, MARFA_NT):
+            raise ValueError(f"cotangent shape {cot.shape} != {(len(P), run.n_sub, MARFA_NT)}")
+        dT = np.zeros(len(P))
+        dP = np.zeros(len(P))
+        dS = np.zeros(self.n_lines)
+        dg = np.zeros(self.n_lines)
+        r = run.c()
+        self._check(self._lib.marfa_vjp(self._h, ctypes.byref(r), P.ctypes.data, T.ctypes.data,
+                                        n.ctypes.data, len(P), cot.ctypes.data, dT.ctypes.data,
+                                        dP.ctypes.data, dS.ctypes.data, dg.ctypes.data))
+        return {"dT": dT, "dP": dP, "dS": dS, "dgamma_air": dg}
+
     def eval_count(self, run: Run, pressure, temperature, density, far=False):
         """Line-shape evaluations of the reference schedule per level (and,
         with far=True, also the part made by the far-line kernel)."""

@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libmarfa_gpu.so"
 CLI = PKG / "marfa"
-SOURCES = ["marfa_kernels.cu", "marfa_api.cu", "marfa_static.cu"]
+SOURCES = ["marfa_kernels.cu", "marfa_adjoint.cu", "marfa_api.cu", "marfa_static.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -44,11 +44,12 @@ struct marfa_ctx {
   float *d_S = nullptr, *d_gair = nullptr, *d_gself = nullptr, *d_elow = nullptr,
         *d_nair = nullptr, *d_delta = nullptr;
   int *d_iso = nullptr;
+  double *d_S64 = nullptr, *d_gair64 = nullptr; // marfa_ctx_set_line_params overrides
   double *d_tips = nullptr;
   int *d_err = nullptr;
   // grow-only work buffers
   DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
-      b_out, b_out64, b_dump, b_count, b_near, b_gstage;
+      b_out, b_out64, b_dump, b_count, b_near, b_gstage, b_aux, b_gscr, b_cot, b_grad;
   std::string err;
   std::vector<cudaEvent_t> events;
   // timing marks of the last compute call: (family, start, stop); family 5
@@ -123,6 +124,7 @@ struct Plan {
   std::vector<int> chunk_sub;
   std::vector<int64_t> chunk_begin, chunk_end;
   std::vector<int> sub_chunk0;    // n_sub + 1
+  int max_chunks = 0;             // most chunks of one subinterval
 };
 
 // Windows of all subintervals; returns 0 or MARFA_E_DB with `bad` = the
@@ -189,6 +191,8 @@ int make_plan(marfa_ctx *ctx, const marfa_run *run, Plan &pl) {
     }
   }
   pl.sub_chunk0[pl.n_sub] = (int)pl.chunk_sub.size();
+  for (int isub = 0; isub < pl.n_sub; ++isub)
+    pl.max_chunks = std::max(pl.max_chunks, pl.sub_chunk0[isub + 1] - pl.sub_chunk0[isub]);
   return MARFA_OK;
 }
 
@@ -237,7 +241,14 @@ int build_levels(marfa_ctx *ctx, int n, const double *P, const double *T, const 
   return MARFA_OK;
 }
 
+// Device buffers of a vector-Jacobian product (marfa_vjp).
+struct VjpOut {
+  const double *cot = nullptr;   // [levels][n_sub][NT] cotangent of the records
+  double *dS = nullptr, *dgair = nullptr, *dT = nullptr, *dP = nullptr;
+};
+
 struct Outputs {
+  const VjpOut *vjp = nullptr;   // adjoint instead of records
   float *host_out = nullptr;     // host records (copied per level chunk)
   double *host_out64 = nullptr;
   float *dev_out = nullptr;      // device records (written in place)
@@ -276,15 +287,17 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   // memory plan: levels per chunk and units per fine/cascade batch
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-  const size_t per_level = (size_t)N * (8 + sizeof(LineGen) + (f64 ? sizeof(Hot64) : sizeof(Hot32)) + 8 + 8 + 4) +
-                           (size_t)C * NFAR * 8 + (size_t)nsub * NT * (o.dev_out ? 0 : 4) +
+  const bool adj = o.vjp != nullptr;
+  const size_t per_level = (size_t)N * (8 + sizeof(LineGen) + (f64 ? sizeof(Hot64) : sizeof(Hot32)) + 8 + 8 + 4 +
+                                        (adj ? sizeof(LineAux) : 0)) +
+                           (size_t)C * NFAR * 8 + (size_t)nsub * NT * (o.dev_out || adj ? 0 : 4) +
                            (o.host_out64 ? (size_t)nsub * NT * 8 : 0);
   const size_t reuse = ctx->b_nus.cap + ctx->b_gen.cap + ctx->b_hot.cap + ctx->b_rank.cap + ctx->b_snu.cap +
                        ctx->b_sidx.cap + ctx->b_far.cap + ctx->b_out.cap + ctx->b_out64.cap;
   const size_t budget = (size_t)((double)(free_b + reuse) * 0.55);
   int Lc = (int)std::max<size_t>(1, std::min<size_t>((size_t)n_levels, budget / std::max<size_t>(per_level, 1)));
   const size_t elem = f64 ? 8 : 4;
-  const size_t unit_bytes = (size_t)SCR_STRIDE * elem;
+  const size_t unit_bytes = (size_t)SCR_STRIDE * elem * (adj ? 2 : 1); // + gradient scratch
   const size_t scr_budget = std::max<size_t>(unit_bytes, std::min<size_t>((size_t)4 << 30, (free_b + ctx->b_scr.cap) / 5));
   int UB = (int)std::max<size_t>(1, std::min<size_t>((size_t)Lc * nsub, scr_budget / unit_bytes));
 
@@ -295,10 +308,14 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   CK(ensure(ctx->b_snu, (size_t)Lc * N * 8), "alloc snu");
   CK(ensure(ctx->b_sidx, (size_t)Lc * N * 4), "alloc sidx");
   CK(ensure(ctx->b_far, (size_t)Lc * std::max(C, 1) * NFAR * 8), "alloc far");
-  CK(ensure(ctx->b_scr, (size_t)UB * unit_bytes), "alloc scratch");
+  CK(ensure(ctx->b_scr, (size_t)UB * SCR_STRIDE * elem), "alloc scratch");
+  if (adj) {
+    CK(ensure(ctx->b_gscr, (size_t)UB * SCR_STRIDE * 8), "alloc gradient scratch");
+    CK(ensure(ctx->b_aux, (size_t)Lc * N * sizeof(LineAux)), "alloc line partials");
+  }
   CK(ensure(ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
   CK(ensure(ctx->b_margin, (size_t)n_levels * 8), "alloc margin");
-  if (!o.dev_out) CK(ensure(ctx->b_out, (size_t)Lc * nsub * NT * 4), "alloc out");
+  if (!o.dev_out && !adj) CK(ensure(ctx->b_out, (size_t)Lc * nsub * NT * 4), "alloc out");
   if (o.host_out64) CK(ensure(ctx->b_out64, (size_t)Lc * nsub * NT * 8), "alloc out64");
   if (o.host_dump) CK(ensure(ctx->b_dump, (size_t)(NT + 3 * NCELLS) * 8), "alloc dump");
   // window and chunk tables
@@ -339,7 +356,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st), "memset err");
 
   WindowTable win{d_s, d_e, d_lo, d_hi, nsub};
-  DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N};
+  DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N,
+                 ctx->d_S64, ctx->d_gair64};
 
   // timing events of every kernel family, resolved by marfa_last_timings
   ctx->marks.clear();
@@ -378,6 +396,19 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     if (e0) cudaEventRecord(e0, st);
     CK(launch_prep(pp, st), "prep kernel");
     ctx->launches += 1;
+    if (adj) {
+      AdjPrepParams ap;
+      ap.lines = dl;
+      ap.tips = ctx->d_tips;
+      ap.n_iso = ctx->n_iso;
+      ap.n_temp = ctx->n_temp;
+      ap.lv = pp.lv;
+      ap.n_levels = nl;
+      ap.c = cst;
+      ap.aux = (LineAux *)ctx->b_aux.p;
+      CK(launch_adjoint_prep(ap, st), "adjoint prep kernel");
+      ctx->launches += 1;
+    }
     if (e1) cudaEventRecord(e1, st);
     SortParams sp;
     sp.nu = ctx->d_nu;
@@ -488,6 +519,51 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       }
       ctx->launches += 1;
       if (f1) cudaEventRecord(f1, st);
+      if (adj) {
+        CascadeAdjParams ca;
+        ca.scratch = (const double *)ctx->b_scr.p;
+        ca.far = fp.out;
+        ca.sub_chunk0 = d_sc0;
+        ca.lv = pp.lv;
+        ca.n_chunks = C;
+        ca.n_sub = nsub;
+        ca.unit0 = u0;
+        ca.n_units = nu_;
+        ca.level_out0 = l0;
+        ca.target = run->target;
+        ca.cot = o.vjp->cot;
+        ca.gscratch = (double *)ctx->b_gscr.p;
+        CK(launch_cascade_adjoint(ca, st), "cascade adjoint kernel");
+        AdjointParams ad;
+        ad.snu = sp.snu;
+        ad.sidx = sp.sidx;
+        ad.nus = pp.nus;
+        ad.gen = pp.gen;
+        ad.aux = (const LineAux *)ctx->b_aux.p;
+        ad.lv = pp.lv;
+        ad.win = win;
+        ad.sub_chunk0 = d_sc0;
+        ad.chunk_begin = d_cb;
+        ad.chunk_end = d_ce;
+        ad.max_chunks = pl.max_chunks;
+        ad.n_lines = N;
+        ad.unit0 = u0;
+        ad.n_units = nu_;
+        ad.level_out0 = l0;
+        ad.cutoff = run->cutoff;
+        ad.c = cst;
+        ad.gscratch = (const double *)ctx->b_gscr.p;
+        ad.dS = o.vjp->dS;
+        ad.dgair = o.vjp->dgair;
+        ad.dT = o.vjp->dT;
+        ad.dP = o.vjp->dP;
+        CK(launch_line_adjoint(ad, chi, std::min(64, (max_near + 255) / 256), st), "line adjoint kernels");
+        ctx->launches += 2 + (pl.max_chunks > 0 ? 1 : 0);
+        if (f2) cudaEventRecord(f2, st);
+        mark(3, f0, f1);
+        mark(4, f1, f2);
+        continue;
+      }
       CascadeParams cp;
       cp.scratch = ctx->b_scr.p;
       cp.far = fp.out;
@@ -665,12 +741,13 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   void *ps[] = {ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta,
-                ctx->d_iso, ctx->d_tips, ctx->d_err};
+                ctx->d_iso, ctx->d_tips, ctx->d_err, ctx->d_S64, ctx->d_gair64};
   for (void *p : ps)
     if (p) cudaFree(p);
   DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
                   &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
-                  &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_near, &ctx->b_gstage};
+                  &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_near, &ctx->b_gstage, &ctx->b_aux,
+                  &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad};
   for (DevBuf *b : bs) release(*b);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -715,6 +792,84 @@ int marfa_compute_device(marfa_ctx *ctx, const marfa_run *run, int n_profiles, c
   try {
     return run_levels(ctx, run, total, pressure, temperature, density, o,
                       stream ? (cudaStream_t)stream : ctx->stream);
+  } catch (...) {
+    return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
+  }
+}
+
+int marfa_ctx_set_line_params(marfa_ctx *ctx, const double *S, const double *gamma_air) {
+  if (!ctx) return MARFA_E_ARG;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "stream sync");
+  const size_t nb = (size_t)ctx->n_lines * 8;
+  auto put = [&](double *&dst, const double *src) -> int {
+    if (!src) {
+      if (dst) cudaFree(dst);
+      dst = nullptr;
+      return MARFA_OK;
+    }
+    for (int64_t i = 0; i < ctx->n_lines; ++i)
+      if (!std::isfinite(src[i])) return set_err(ctx, MARFA_E_ARG, "line %lld: non-finite value", (long long)i);
+    if (!dst) CK(cudaMalloc(&dst, nb), "alloc line overrides");
+    CK(cudaMemcpy(dst, src, nb, cudaMemcpyHostToDevice), "h2d line overrides");
+    return MARFA_OK;
+  };
+  int rc = put(ctx->d_S64, S);
+  if (!rc) rc = put(ctx->d_gair64, gamma_air);
+  if (rc) return rc;
+  // the intensity scale of the FP32-compensated form follows the largest S
+  double smax = 0.0;
+  if (S) {
+    for (int64_t i = 0; i < ctx->n_lines; ++i) smax = std::max(smax, std::fabs(S[i]));
+  } else {
+    std::vector<float> Sf(ctx->n_lines);
+    CK(cudaMemcpy(Sf.data(), ctx->d_S, (size_t)ctx->n_lines * 4, cudaMemcpyDeviceToHost), "d2h S");
+    for (float v : Sf) smax = std::max(smax, (double)std::fabs(v));
+  }
+  ctx->smax = smax;
+  return MARFA_OK;
+}
+
+int marfa_vjp(marfa_ctx *ctx, const marfa_run *run, const double *pressure, const double *temperature,
+              const double *density, int n_levels, const double *cotangent, double *d_temperature,
+              double *d_pressure, double *d_S, double *d_gamma_air) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!run || !cotangent || !d_temperature || !d_pressure || !d_S || !d_gamma_air)
+    return set_err(ctx, MARFA_E_ARG, "null argument");
+  if (run->shape != MARFA_SHAPE_VOIGT) return set_err(ctx, MARFA_E_ARG, "the adjoint needs the Voigt shape");
+  if (n_levels < 1) return set_err(ctx, MARFA_E_ARG, "no levels");
+  if (n_levels > 200) return set_err(ctx, 6, "%d levels > 200", n_levels);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+  marfa_run r = *run;
+  r.precision = MARFA_PREC_FP64;
+  int rc = check_run(ctx, &r);
+  if (rc) return rc;
+  const int nsub = marfa_num_subintervals(r.start_wv, r.end_wv);
+  const int64_t N = ctx->n_lines;
+  cudaStream_t st = ctx->stream;
+  try {
+    const size_t ncot = (size_t)n_levels * nsub * NT;
+    CK(ensure(ctx->b_cot, std::max<size_t>(ncot, 1) * 8), "alloc cotangent");
+    CK(ensure(ctx->b_grad, ((size_t)2 * N + 2 * n_levels) * 8), "alloc gradients");
+    double *g = (double *)ctx->b_grad.p;
+    VjpOut v;
+    v.cot = (const double *)ctx->b_cot.p;
+    v.dS = g;
+    v.dgair = g + N;
+    v.dT = g + 2 * N;
+    v.dP = g + 2 * N + n_levels;
+    if (ncot) CK(cudaMemcpyAsync(ctx->b_cot.p, cotangent, ncot * 8, cudaMemcpyHostToDevice, st), "h2d cotangent");
+    CK(cudaMemsetAsync(g, 0, ((size_t)2 * N + 2 * n_levels) * 8, st), "memset gradients");
+    Outputs o;
+    o.vjp = &v;
+    rc = run_levels(ctx, &r, n_levels, pressure, temperature, density, o, st);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(d_S, v.dS, (size_t)N * 8, cudaMemcpyDeviceToHost, st), "d2h dS");
+    CK(cudaMemcpyAsync(d_gamma_air, v.dgair, (size_t)N * 8, cudaMemcpyDeviceToHost, st), "d2h dgamma");
+    CK(cudaMemcpyAsync(d_temperature, v.dT, (size_t)n_levels * 8, cudaMemcpyDeviceToHost, st), "d2h dT");
+    CK(cudaMemcpyAsync(d_pressure, v.dP, (size_t)n_levels * 8, cudaMemcpyDeviceToHost, st), "d2h dP");
+    CK(cudaStreamSynchronize(st), "stream sync");
+    return MARFA_OK;
   } catch (...) {
     return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
   }
@@ -768,7 +923,8 @@ int marfa_eval_count(marfa_ctx *ctx, const marfa_run *run, int n_levels, const d
     CK(cudaMemcpyAsync(ctx->b_lv.p, lv.data(), n_levels * sizeof(LevelConst), cudaMemcpyHostToDevice, st), "h2d");
     CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st), "memset");
     std::vector<unsigned long long> cnt(2 * (size_t)C);
-    DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N};
+    DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N,
+                 ctx->d_S64, ctx->d_gair64};
     for (int l = 0; l < n_levels; ++l) {
       PrepParams pp{};
       pp.lines = dl;

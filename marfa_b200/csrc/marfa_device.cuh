@@ -311,4 +311,60 @@ __device__ __forceinline__ Real voigt_general(double Xd, const LineGen &g, const
   return voigt_core<Real, CHI>(Xd, sp.qx, sp.vy, sp.lorA, sp.g2, sp.hum, lv.perrin_b1, lv.perrin_b2, c.sqrt14);
 }
 
+// Classification of one line against subinterval [s, se] (LBL.f90:81-98 and
+// the first tests of leftLBL / rightLBL): returns the distance D >= 1 from
+// the line to the nearest grid-0 position and whether the line sits left of
+// the subinterval; false when the line is near, inside or beyond the cutoff.
+__device__ __forceinline__ bool far_line(double nu, double s, double se, double cut, double &D,
+                                         bool &left) {
+  if (nu < s) {
+    D = -(nu - s);
+    left = true;
+    return !(D > cut) && !(D < 1.0);
+  }
+  if (nu > se) {
+    D = (nu - s) - DELTA_WV;
+    left = false;
+    return !(D >= cut) && !(D < 1.0);
+  }
+  return false;
+}
+
+// upper end of the UU (or V) interval of centre lines that walk over cell j
+// of grid k: (2*floor((j+1)/2) + 2) * H_k  (derived from LineGridCalc.f90:202-331)
+__device__ __forceinline__ double walk_hi(int j, double hk) { return (double)(2 * ((j + 1) / 2) + 2) * hk; }
+
+// Bounds of the near lines of subinterval [s, se] in a level's shifted-centre
+// order: which = 0 first line with nu' > s - 1 (or inside), 1 first with
+// nu' >= s, 2 first with nu' > se, 3 first line at least 1 cm-1 right of the
+// subinterval.  [b0, b1) near-left, [b1, b2) centre, [b2, b3) near-right.
+__device__ __forceinline__ int64_t near_bound(const double *snu, int64_t n, double s, double se, int which) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t m = (lo + hi) >> 1;
+    const double v = snu[m];
+    bool pr;
+    if (which == 0) pr = !(v < s && (v - s) <= -1.0);
+    else if (which == 1) pr = v >= s;
+    else if (which == 2) pr = v > se;
+    else pr = v > se && ((v - s) - DELTA_WV) >= 1.0;
+    if (pr) hi = m; else lo = m + 1;
+  }
+  return lo;
+}
+
+// Whether near line `li` (shifted centre v) contributes to the subinterval:
+// inside the line window, within the cutoff (left side keeps D == cutoff,
+// right side drops it: LineGridCalc.f90:23, 509), centre lines with UU < 10.
+// Sets UU = v - s and the class (0 near-left, 1 centre, 2 near-right).
+__device__ __forceinline__ bool near_keep(double v, int64_t li, double s, double se, double cut, int64_t wlo,
+                                          int64_t whi, double &UU, int &cls) {
+  UU = v - s;
+  cls = 1;
+  if (li < wlo || li >= whi) return false;
+  if (v < s) { cls = 0; return -UU <= cut; }
+  if (v > se) { cls = 2; return (UU - DELTA_WV) < cut; }
+  return UU < DELTA_WV;
+}
+
 } // namespace marfa

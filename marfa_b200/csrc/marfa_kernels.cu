@@ -47,8 +47,9 @@ __global__ void __launch_bounds__(256) prep_kernel(PrepParams p) {
   // shiftedLinePosition, dopplerHWHM, lorentzHWHM (Spectroscopy.f90:38-88)
   const double nus = nu + (double)p.lines.delta[i] * P;
   const double alpha = c.doppler * nus * sqrt(T / M);
+  const double gair = p.lines.gair64 ? p.lines.gair64[i] : (double)p.lines.gair[i];
   const double gamma = pow(c.tref / T, (double)p.lines.nair[i]) *
-                       ((double)p.lines.gair[i] * (P - lv.pself) + (double)p.lines.gself[i] * lv.pself);
+                       (gair * (P - lv.pself) + (double)p.lines.gself[i] * lv.pself);
   // TIPSofT (Spectroscopy.f90:91-115): linear interpolation in 2 K steps
   const double tval = (T - 20.0) / 2.0 + 1.0;
   const int idx = (int)tval;
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(256) prep_kernel(PrepParams p) {
     const double E = (double)p.lines.elow[i];
     const double boltz = exp(-(c.c2 * E / T)) / exp(-(c.c2 * E / c.tref));
     const double emis = (1.0 - exp(-(c.c2 * nu / T))) / (1.0 - exp(-(c.c2 * nu / c.tref)));
-    S = (double)p.lines.S[i] * (Qref / Q) * boltz * emis;
+    S = (p.lines.S64 ? p.lines.S64[i] : (double)p.lines.S[i]) * (Qref / Q) * boltz * emis;
   }
   LineGen g;
   g.qx = c.sqln2 / alpha;
@@ -162,25 +163,6 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[N], double *dst) 
 }
 
 // ---------------------------------------------------------------- far lines
-// Classification of one line against subinterval [s, se] (LBL.f90:81-98 and
-// the first tests of leftLBL / rightLBL): returns the distance D >= 1 from
-// the line to the nearest grid-0 position and whether the line sits left of
-// the subinterval; false when the line is near, inside or beyond the cutoff.
-__device__ __forceinline__ bool far_line(double nu, double s, double se, double cut, double &D,
-                                         bool &left) {
-  if (nu < s) {
-    D = -(nu - s);
-    left = true;
-    return !(D > cut) && !(D < 1.0);
-  }
-  if (nu > se) {
-    D = (nu - s) - DELTA_WV;
-    left = false;
-    return !(D >= cut) && !(D < 1.0);
-  }
-  return false;
-}
-
 // First grid-0 position index k (0..21) whose distance D + k/2 passes the
 // chi-factor boundary b (strictly when `strict`), decided in double.
 __device__ __forceinline__ int first_k_past(double D, double b, bool strict) {
@@ -459,9 +441,6 @@ struct NearStore {
   }
 };
 
-// upper end of the UU (or V) interval of centre lines that walk over cell j
-// of grid k: (2*floor((j+1)/2) + 2) * H_k  (derived from LineGridCalc.f90:202-331)
-__device__ __forceinline__ double walk_hi(int j, double hk) { return (double)(2 * ((j + 1) / 2) + 2) * hk; }
 
 // Grid-0 and RK(1) contributions of one near line: leftLBL grid-0 cells 2..10
 // (near-left), centerLBL walks (centre), rightLBL cells 9..1 (near-right).
@@ -771,22 +750,8 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
   const int64_t wlo = p.win.lo[sub], whi = p.win.hi[sub];
   __shared__ int64_t sb[4];
   __shared__ int s_counts[2];
-  if (threadIdx.x < 4) {
-    // [a, c0): near-left; [c0, c1): centre; [c1, b): near-right (sorted order)
-    const int64_t n = p.n_lines;
-    int64_t lo = 0, hi = n;
-    while (lo < hi) {
-      const int64_t m = (lo + hi) >> 1;
-      const double v = snu[m];
-      bool pr;
-      if (threadIdx.x == 0) pr = !(v < s && (v - s) <= -1.0);
-      else if (threadIdx.x == 1) pr = v >= s;
-      else if (threadIdx.x == 2) pr = v > se;
-      else pr = v > se && ((v - s) - DELTA_WV) >= 1.0;
-      if (pr) hi = m; else lo = m + 1;
-    }
-    sb[threadIdx.x] = lo;
-  }
+  // [a, c0): near-left; [c0, c1): centre; [c1, b): near-right (sorted order)
+  if (threadIdx.x < 4) sb[threadIdx.x] = near_bound(snu, p.n_lines, s, se, threadIdx.x);
   if (threadIdx.x < 2) s_counts[threadIdx.x] = 0;
   __syncthreads();
   const int64_t a = sb[0], c0 = sb[1], c1 = sb[2], b = sb[3];
@@ -818,13 +783,7 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
     int64_t li = 0;
     if (q < b) {
       li = sidx[q];
-      const double v = snu[q];
-      UU = v - s;
-      if (li >= wlo && li < whi) {
-        if (v < s) { cls = 0; keep = -UU <= cut; }
-        else if (v > se) { cls = 2; keep = (UU - DELTA_WV) < cut; }
-        else keep = UU < DELTA_WV;
-      }
+      keep = near_keep(snu[q], li, s, se, cut, wlo, whi, UU, cls);
     }
     int tot;
     const int pos = m_total + block_excl_scan(keep, tot);

@@ -12,6 +12,8 @@ struct DeviceLines {
   const float *S, *gair, *gself, *elow, *nair, *delta;
   const int *iso; // jointMolIso / 100
   int64_t n;
+  const double *S64 = nullptr;    // optional double overrides of S and gamma_air
+  const double *gair64 = nullptr; // (set by marfa_ctx_set_line_params)
 };
 
 struct PrepParams {
@@ -113,6 +115,66 @@ struct CountParams {
   double cutoff;
   unsigned long long *out;       // [Lc][C]
 };
+
+// ------------------------------------------------------------ adjoint
+// Partial derivatives of the per-(level, line) spectroscopy.
+struct LineAux {
+  double ratio;    // S(T) / S_ref
+  double dlnS_dT;  // d ln S(T) / dT
+  double dg_dT;    // d gamma_L / dT (pself grows with T at fixed density)
+  double dg_dP;    // d gamma_L / dP
+  double dg_dgair; // d gamma_L / d gamma_air
+  double delta;    // pressure shift: d nu' / dP
+};
+
+struct AdjPrepParams {
+  DeviceLines lines;
+  const double *tips;
+  int n_iso, n_temp;
+  const LevelConst *lv;
+  int n_levels;
+  Consts c;
+  LineAux *aux;                  // [Lc][N]
+};
+
+struct CascadeAdjParams {
+  const double *scratch;         // FP64 accumulators of the batch
+  const double *far;             // [Lc][C][NFAR]
+  const int *sub_chunk0;
+  const LevelConst *lv;
+  int n_chunks, n_sub;
+  int unit0, n_units;
+  int level_out0;
+  int target;
+  const double *cot;             // [levels][n_sub][NT] cotangent of the records
+  double *gscratch;              // [n_units][SCR_STRIDE] dL / d accumulator
+};
+
+struct AdjointParams {
+  const double *snu;
+  const int *sidx;
+  const double *nus;
+  const LineGen *gen;
+  const LineAux *aux;
+  const LevelConst *lv;
+  WindowTable win;
+  const int *sub_chunk0;
+  const int64_t *chunk_begin, *chunk_end;
+  int max_chunks;                // most far-kernel chunks of one subinterval
+  int64_t n_lines;
+  int unit0, n_units;
+  int level_out0;
+  double cutoff;
+  Consts c;
+  const double *gscratch;
+  double *dS, *dgair;            // [N] per-line gradients (accumulated)
+  double *dT, *dP;               // [levels]
+};
+
+// launchers (marfa_adjoint.cu)
+cudaError_t launch_adjoint_prep(const AdjPrepParams &p, cudaStream_t st);
+cudaError_t launch_cascade_adjoint(const CascadeAdjParams &p, cudaStream_t st);
+cudaError_t launch_line_adjoint(const AdjointParams &p, int chi, int near_blocks, cudaStream_t st);
 
 // launchers (marfa_kernels.cu)
 cudaError_t launch_prep(const PrepParams &p, cudaStream_t st);
