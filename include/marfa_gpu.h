@@ -209,7 +209,7 @@ int marfa_last_timings(marfa_ctx *ctx, double *times);
  * same array: calls that overlap on the GPU race. */
 #define MARFA_STATIC_MAX_WINDOW_LINES 65536
 #define MARFA_STATIC_MAX_NEAR_LINES 8192
-#define MARFA_STATIC_SCRATCH_BYTES (11u * 1024u * 1024u)
+#define MARFA_STATIC_SCRATCH_BYTES (12u * 1024u * 1024u)
 int marfa_compute_record_static(const marfa_line_record *lines, int64_t n_lines, const double *tips,
                                 int n_iso, int n_temp, const marfa_run *run, double pressure,
                                 double temperature, double density, int isub, float *record,

@@ -49,7 +49,7 @@ struct marfa_ctx {
   int *d_err = nullptr;
   // grow-only work buffers
   DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
-      b_out, b_out64, b_dump, b_count, b_near, b_gstage, b_aux, b_gscr, b_cot, b_grad;
+      b_out, b_out64, b_dump, b_count, b_near, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order;
   std::string err;
   std::vector<cudaEvent_t> events;
   // timing marks of the last compute call: (family, start, stop); family 5
@@ -469,7 +469,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.err = ctx->d_err;
     fn.phase_clock = nullptr;
     // diagnostics: MARFA_PHASE_CLOCK=<file> records clock64 marks of every
-    // fine-kernel block of the first batch (int64 [units][10]: phase marks, near count, per-family run cycles) into <file>
+    // fine-kernel block of the first batch (int64 [units][10]: start, staged, grid 0, grids 1-3, end, near count, grids 4-6, grids 7-9, line-half and site-half cycles) into <file>
     const char *clock_path = std::getenv("MARFA_PHASE_CLOCK");
     if (clock_path && l0 == 0) {
       CK(ensure(ctx->b_count, (size_t)units * 10 * 8), "alloc clock");
@@ -485,27 +485,46 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     CK(cudaMemcpyAsync(ncount.data(), ctx->b_near.p, (size_t)units * 4, cudaMemcpyDeviceToHost, st), "d2h near");
     CK(cudaStreamSynchronize(st), "sync near");
     const int max_near = units ? *std::max_element(ncount.begin(), ncount.end()) : 0;
-    // two blocks per SM fit when each stages at most ~100 KB of lines
-    const int smem_max = f64 ? 4096 : 2816;
+    // staged lines per block in shared memory; units with more near lines
+    // stage in a global slice of their block
+    const int smem_max = f64 ? 4096 : 2688;
     fn.smem_cap = std::max(256, std::min(smem_max, (max_near + 127) / 128 * 128));
     fn.gstage = nullptr;
-    fn.gstage_cap = 0;
-    fn.gstage_bytes = 0;
-    int UBc = UB;
-    if (max_near > fn.smem_cap) {
-      fn.gstage_cap = (max_near + 255) / 256 * 256;
-      fn.gstage_bytes = fine_smem_bytes(fn.gstage_cap, f64);
-      const size_t room = std::max<size_t>(fn.gstage_bytes, (size_t)1 << 30);
-      UBc = (int)std::max<size_t>(1, std::min<size_t>((size_t)UB, room / fn.gstage_bytes));
-      CK(ensure(ctx->b_gstage, (size_t)UBc * fn.gstage_bytes), "alloc staging");
+    fn.gstage_cap = max_near > fn.smem_cap ? (max_near + 255) / 256 * 256 : 0;
+    fn.gstage_bytes = fn.gstage_cap ? fine_smem_bytes(fn.gstage_cap, f64) : 0;
+    int resident = 0;
+    CK(fine_plan(run->precision, chi, fn.smem_cap, &fn.vsm_rows, &resident), "fine occupancy");
+    if (fn.gstage_cap) {
+      CK(ensure(ctx->b_gstage, (size_t)resident * fn.gstage_bytes), "alloc staging");
       fn.gstage = ctx->b_gstage.p;
     }
+    fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
+    fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
+    CK(ensure(ctx->b_vbuf, (size_t)resident * fn.vbuf_stride * elem), "alloc slot buffers");
+    fn.vbuf = ctx->b_vbuf.p;
+    CK(ensure(ctx->b_queue, 256), "alloc queue");
+    fn.queue = (int *)ctx->b_queue.p;
+    // work order of every batch: most near lines first
+    const int UBc = UB;
+    std::vector<int> order(units);
+    for (int u0 = 0; u0 < units; u0 += UBc) {
+      const int nu_ = std::min(UBc, units - u0);
+      for (int i = 0; i < nu_; ++i) order[u0 + i] = i;
+      std::stable_sort(order.begin() + u0, order.begin() + u0 + nu_,
+                       [&](int x, int y) { return ncount[u0 + x] > ncount[u0 + y]; });
+    }
+    CK(ensure(ctx->b_order, (size_t)units * 4), "alloc order");
+    CK(cudaMemcpyAsync(ctx->b_order.p, order.data(), (size_t)units * 4, cudaMemcpyHostToDevice, st), "h2d order");
+    CK(cudaStreamSynchronize(st), "sync order"); // `order` is a host temporary
     for (int u0 = 0; u0 < units; u0 += UBc) {
       const int nu_ = std::min(UBc, units - u0);
       fn.unit0 = u0;
       fn.n_units = nu_;
+      fn.order = (const int *)ctx->b_order.p + u0;
+      fn.grid = std::min(resident, nu_);
       cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
       if (f0) cudaEventRecord(f0, st);
+      CK(cudaMemsetAsync(fn.queue, 0, sizeof(int), st), "memset queue");
       CK(launch_fine(fn, run->precision, chi, st), "fine kernel");
       if (fn.phase_clock) {
         std::vector<long long> pcv((size_t)nu_ * 10);
@@ -747,7 +766,7 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
   DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
                   &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
                   &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_near, &ctx->b_gstage, &ctx->b_aux,
-                  &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad};
+                  &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order};
   for (DevBuf *b : bs) release(*b);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -421,22 +421,27 @@ struct NearStore {
   }
   // first[b] = first centre line with floor(UU * 2^8) >= b, b = 0 .. NBUCKET
   const int *first;
-  // centre lines: first q with UU >= x (start from the bucket of x, exact
-  // because the bucket width is a power of two)
-  __device__ __forceinline__ int lb_uu(int, double x) const {
-    int b = (int)floor(x * BUCKETS_PER_CM);
+  // centre lines: floor(UU * 2^11) and floor(V * 2^11), V = fl(10 - UU); the
+  // bin of grid k is the value shifted right by 11 - k
+  const short *n11, *nv11;
+  // first centre line with UU >= a H_k (bin_k >= a)
+  __device__ __forceinline__ int lbL(int k, int a) const {
+    int b = k <= 8 ? (a << (8 - k)) : (a >> (k - 8));
     b = b < 0 ? 0 : (b > NBUCKET ? NBUCKET : b);
     int q = first[b];
-    while (q < c1 && uu[q] < x) ++q;
+    const int sh = 11 - k;
+    while (q < c1 && (n11[q] >> sh) < a) ++q;
     return q;
   }
-  // centre lines: first q with V = 10 - UU < y (one bucket of margin below
-  // 10 - y covers the rounding of V)
-  __device__ __forceinline__ int lb_v(int, double y) const {
-    int b = (int)floor((DELTA_WV - y) * BUCKETS_PER_CM) - 1;
+  // first centre line with V < a H_k (V bin_k < a); one bucket of margin
+  // below 10 - a H_k covers the rounding of V
+  __device__ __forceinline__ int lbV(int k, int a) const {
+    const int t = k <= 8 ? (a << (8 - k)) : ((a + (1 << (k - 8)) - 1) >> (k - 8));
+    int b = NBUCKET - t - 1;
     b = b < 0 ? 0 : (b > NBUCKET ? NBUCKET : b);
     int q = first[b];
-    while (q < c1 && !(DELTA_WV - uu[q] < y)) ++q;
+    const int sh = 11 - k;
+    while (q < c1 && (nv11[q] >> sh) >= a) ++q;
     return q;
   }
 };
@@ -499,7 +504,6 @@ __device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Lane
   }
 }
 
-// One edge site e of grid k (1..9): L(e) and P(e+1).
 // Sum over the lanes of a warp (lane 0 gets the total) when `coop`.
 __device__ __forceinline__ double coop_sum(double v, bool coop) {
   if (coop) {
@@ -509,85 +513,321 @@ __device__ __forceinline__ double coop_sum(double v, bool coop) {
   return v;
 }
 
-// Sites are processed either by one thread (lane 0, stride 1) or by a whole
-// warp whose lanes stride over the contributing lines (coop).
+// ----------------------------------------------------------- fine grids
+// Grids 1..9 and the direct finest points are computed in ten passes (one
+// per grid, then the finest points).  Each pass has two halves:
+//   line half  one thread per near line evaluates every cell of the pass's
+//              grid that the line's walk visits (centerLBL, and the fine
+//              parts of leftLBL / rightLBL).  The line's Kuntz coefficients
+//              are computed once per pass; every evaluation picks its
+//              region's set by selects, without branching.  Values go to a
+//              slot buffer (shared memory when it fits, else an L2-resident
+//              per-block slice), slot = position of the cell relative to
+//              the line.
+//   site half  one thread (a warp on the coarse grids) per accumulator sums
+//              the values of its contiguous runs of lines, in line order.
+// Both halves apply the same placement conditions (derived from
+// LineGridCalc.f90:7-674), from the line's side and from the site's side,
+// as integer comparisons of the lines' bins: with n = floor(UU / H_k) and W
+// an integer, UU >= a H_k <=> n >= a and UU < W H_k <=> n < W (likewise for
+// V = fl(10 - UU) and its bin).  Per accumulator the order of summation is:
+// centre lines of the left walk, centre lines of the right walk, near-left
+// lines, near-right lines, each in ascending shifted-centre order.
+constexpr int FINE_THREADS = 512;
+constexpr int COOP_K = 3; // grids 1..COOP_K: one warp per site in the site half
+__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
+
+// Line shape of one near line for the fine passes: region 0 inline, Kuntz
+// regions 1-3 as one rational form with the line's coefficients selected by
+// region, region 4 through voigt_core.
 template <bool F64, int CHI>
-__device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL, int &curR, void *scr,
-                               int lane, int stride) {
+struct LineEval {
+  using Real = typename std::conditional<F64, double, float>::type;
+  double qx, vy;
+  Real lorA, g2, hum;
+  Real A1, B1, A2, B2;                         // region 1 (Shapes.f90:63-70)
+  Real A3, B3, C3, D3, A4, B4, C4, D4;         // region 2 (Shapes.f90:72-86)
+  Real A5, B5, C5, D5, E5, A6, B6, C6, D6, E6; // region 3 (Shapes.f90:88-113)
+
+  __device__ __forceinline__ void init(const NearStore<F64> &st, int q) {
+    qx = st.qx[q];
+    vy = st.vy[q];
+    lorA = st.lorA[q];
+    g2 = st.g2[q];
+    hum = st.hum[q];
+    const Real Y = (Real)(qx < 0.0 ? 0.0 : vy), Y2 = Y * Y;
+    A1 = ((Real)0.2820948 + (Real)0.5641896 * Y2) * Y;
+    B1 = (Real)0.5641896 * Y;
+    A2 = (Real)0.25 + Y2 + Y2 * Y2;
+    B2 = Y2 + Y2 - (Real)1.;
+    A3 = Y * horner<Real>(Y2, 0.56419, 3.10304, 4.65456, 1.05786);
+    B3 = Y * horner<Real>(Y2, 1.69257, 0.56419, 2.962);
+    C3 = Y * ((Real)1.69257 * Y2 - (Real)2.53885);
+    D3 = Y * (Real)0.56419;
+    A4 = horner<Real>(Y2, 1.0, 6.0, 10.5, 4.5, 0.5625);
+    B4 = horner<Real>(Y2, 4.0, 6.0, 9.0, -4.5);
+    C4 = (Real)10.5 + (Real)6.0 * (Y2 - (Real)1.0) * Y2;
+    D4 = (Real)4.0 * Y2 - (Real)6.0;
+    A5 = horner<Real>(Y, 0.564224, 7.55895, 49.5213, 204.510, 581.746, 1174.8, 1678.33, 1629.76, 973.778,
+                      272.102);
+    B5 = horner<Real>(Y, 2.25689, 22.6778, 100.705, 247.198, 336.364, 220.843, -2.34403, -60.5644);
+    C5 = horner<Real>(Y, 3.38534, 22.6798, 52.8454, 42.5683, 18.546, 4.58029);
+    D5 = horner<Real>(Y, 2.25689, 7.56186, 1.66203, -0.128922);
+    E5 = horner<Real>(Y, 0.564224, 0.971457E-3);
+    A6 = horner<Real>(Y, 1.0, 13.3988, 88.2674, 369.199, 1074.41, 2256.98, 3447.63, 3764.97, 2802.87, 1280.83,
+                      272.102);
+    B6 = horner<Real>(Y, 5., 53.5952, 266.299, 793.427, 1549.68, 2037.31, 1758.34, 902.306, 211.678);
+    C6 = horner<Real>(Y, 10., 80.3928, 269.292, 479.258, 497.302, 308.186, 78.866);
+    D6 = horner<Real>(Y, 10., 53.5952, 92.7586, 55.0293, 22.0353);
+    E6 = horner<Real>(Y, 5.0, 13.3988, 1.49645);
+  }
+
+  __device__ __forceinline__ Real operator()(double X, const LevelConst &lv, double sqrt14) const {
+    const double ax = fabs(X);
+    if (qx < 0.0) return vy < 0.0 ? (Real)1 : (Real)ax; // diagnostic shapes
+    const double VXd = ax * qx;
+    if (VXd >= 15.0) {
+      const Real axr = (Real)ax;
+      const Real lor = fast_div(lorA, axr * axr + g2);
+      if (CHI == CHI_NONE) return lor;
+      if (sizeof(Real) == 8) return lor * (Real)chi_factor_d<CHI>(ax, lv);
+      return lor * (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
+    }
+    const double sum = VXd + vy;
+    const bool r1 = sum >= 15.0, r2 = !r1 && sum >= 5.5;
+    if (!r1 && !r2 && !(VXd <= 1.0 || vy >= 0.02))
+      return voigt_core<Real, CHI>(X, qx, vy, lorA, g2, hum, lv.perrin_b1, lv.perrin_b2, sqrt14);
+    const Real VX = (Real)VXd;
+    const Real x = VX * VX;
+    const Real z = (Real)0, o = (Real)1;
+    const Real n0 = (r1 || r2) ? z : E5;
+    const Real n1 = r1 ? z : (r2 ? D3 : D5);
+    const Real n2 = r1 ? z : (r2 ? C3 : C5);
+    const Real n3 = r1 ? B1 : (r2 ? B3 : B5);
+    const Real n4 = r1 ? A1 : (r2 ? A3 : A5);
+    const Real d0 = (r1 || r2) ? z : o;
+    const Real d1 = r1 ? z : (r2 ? o : E6);
+    const Real d2 = r1 ? z : (r2 ? D4 : D6);
+    const Real d3 = r1 ? o : (r2 ? C4 : C6);
+    const Real d4 = r1 ? B2 : (r2 ? B4 : B6);
+    const Real d5 = r1 ? A2 : (r2 ? A4 : A6);
+    const Real num = (((n0 * x + n1) * x + n2) * x + n3) * x + n4;
+    const Real den = ((((d0 * x + d1) * x + d2) * x + d3) * x + d4) * x + d5;
+    return fast_div(num, den) * hum;
+  }
+};
+
+// Exact int -> double for |n| < 2^51 without the conversion unit: the
+// integer is added into the mantissa of 1.5 * 2^52 and the bias removed.
+__device__ __forceinline__ double i2d(int n) {
+  return __longlong_as_double(0x4338000000000000LL + (long long)n) - 6755399441055744.0;
+}
+
+// Line half of pass k (1..9: grid k; 10: finest points) for staged line q.
+// The offsets X are exact: UU - e H_k is a multiple of the ulp of UU not
+// larger than UU, and so are its neighbours e -+ 1 built from it.
+template <bool F64, int CHI>
+__device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearStore<F64>::Real *vb, int cap) {
+  LineEval<F64, CHI> ev;
+  const double UU = st.uu[q];
+  const int cls = q < st.c0 ? 0 : (q < st.c1 ? 1 : 2);
+  auto put = [&](int slot, double X) { vb[(size_t)slot * cap + q] = ev(X, st.lv, st.sqrt14); };
+  if (k <= 9) {
+    const double hk = h_k(k), hk1 = h_k(k - 1), hn = h_k(k + 1);
+    const int ntk = nt_k(k);
+    if (cls == 1) {
+      const int n = st.n11[q] >> (11 - k);
+      const int nv = st.nv11[q] >> (11 - k);
+      const double V = DELTA_WV - UU;
+      const double bL = UU - i2d(n - 1) * hk; // X of edge n-1
+      const double bV = V - i2d(nv - 1) * hk; // X of the right-walk edge with rP = nv-1
+      bool any = false;
+      bool te[3], tm[2], re[3], rm[2];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) { // left walk, edge e = n-1-d: L(e) and/or P(e+1)
+        const int e = n - 1 - d;
+        const bool tl = e >= 1 && e <= ntk && n < 2 * ((e + 1) / 2) + 2;
+        const bool tp = e >= 0 && e <= ntk - 1 && d >= 1 && n < 2 * ((e + 2) / 2) + 2;
+        te[d] = tl || tp;
+        any |= te[d];
+      }
+#pragma unroll
+      for (int d = 0; d < 2; ++d) { // left walk, mid m = n-1-d
+        const int m = n - 1 - d;
+        tm[d] = m >= 1 && m <= ntk && n < 2 * ((m + 1) / 2) + 2;
+        any |= tm[d];
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) { // right walk, edge e = ntk-nv+1+d (rP = nv-1-d, rL = rP+1)
+        const int e = ntk - nv + 1 + d, rP = nv - 1 - d, rL = rP + 1;
+        const bool tl = e >= 1 && e <= ntk && nv >= rL + 1 && nv < 2 * ((rL + 1) / 2) + 2;
+        const bool tp = e >= 0 && e <= ntk - 1 && nv < 2 * ((rP + 1) / 2) + 2;
+        re[d] = tl || tp;
+        any |= re[d];
+      }
+#pragma unroll
+      for (int d = 0; d < 2; ++d) { // right walk, mid m = ntk+2-nv+d (r = nv-1-d)
+        const int m = ntk + 2 - nv + d, r = nv - 1 - d;
+        rm[d] = m >= 1 && m <= ntk && nv < 2 * ((r + 1) / 2) + 2;
+        any |= rm[d];
+      }
+      if (!any) return;
+      ev.init(st, q);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (te[d]) put(d, bL + (double)d * hk);
+#pragma unroll
+      for (int d = 0; d < 2; ++d)
+        if (tm[d]) put(3 + d, (bL + (double)d * hk) + hn);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (re[d]) put(5 + d, bV + (double)d * hk);
+#pragma unroll
+      for (int d = 0; d < 2; ++d)
+        if (rm[d]) put(8 + d, (bV + (double)d * hk) + hn);
+    } else if (cls == 0) {
+      if (UU > -hk1) { // D = -UU < H_{k-1}: cells 1 and 2 (leftLBL labels 20-28, 121-129)
+        ev.init(st, q);
+        const bool own = -UU >= hk;
+        if (own) put(0, UU);      // e = 0: P(1)
+        put(1, UU - hk);          // e = 1: L(1) when own, P(2)
+        put(2, UU - hk1);         // e = 2: L(2)
+        if (own) put(3, UU - hn); // M(1)
+        put(4, (UU - hk) - hn);   // M(2)
+      }
+    } else {
+      const double U = UU - DELTA_WV;
+      if (U < hk1) { // cells ntk and ntk-1 (rightLBL labels 60-69, 131-139)
+        ev.init(st, q);
+        const bool own = U >= hk;
+        if (own) put(0, U);       // e = ntk: L(ntk)
+        put(1, U + hk);           // e = ntk-1: L(ntk-1), P(ntk) when own
+        put(2, U + hk1);          // e = ntk-2: P(ntk-1)
+        if (own) put(3, U + hn);  // M(ntk)
+        put(4, (U + hk) + hn);    // M(ntk-1)
+      }
+    }
+  } else {
+    const double H = HSTEP, H9 = h_k(9);
+    if (cls == 1) {
+      ev.init(st, q);
+      const int ni = st.n11[q], nv9 = st.nv11[q] >> 2;
+      const double b0 = UU - i2d(ni) * H; // in [0, H)
+#pragma unroll
+      for (int d = 0; d < 7; ++d) { // left fine loop (LineGridCalc.f90:332-339): i = ni+1-d
+        const int i = ni + 1 - d;
+        if (i >= 2 && i <= NT && ni < 4 * ((i - 2) / 4) + 8) put(d, b0 + (double)d * H);
+      }
+#pragma unroll
+      for (int d = 0; d < 8; ++d) { // right fine loop (LineGridCalc.f90:485-490): i = ni+2+d
+        const int i = ni + 2 + d;
+        if (i >= 2 && i <= NT && nv9 < (NT - i) / 4 + 2) put(7 + d, b0 - (double)(1 + d) * H);
+      }
+    } else if (cls == 0) {
+      if (UU > -H9) { // leftLBL label 29: RK(2..5)
+        ev.init(st, q);
+        put(0, UU - H);
+        put(1, (UU - H) - H);
+        put(2, (UU + H) - H9);
+        put(3, UU - H9);
+      }
+    } else {
+      const double U = UU - DELTA_WV;
+      if (U < H9) { // rightLBL label 69: RK(NT..NT-3)
+        ev.init(st, q);
+        put(0, U);
+        put(1, U + H);
+        put(2, (U + H) + H);
+        put(3, (U + H9) - H);
+      }
+    }
+  }
+}
+
+// The site half reads the slot values of up to GB lines per batch, loads
+// first, sums after, so that the loads of a batch are in flight together.
+constexpr int GB = 4;
+
+// Site half: edge e (0..ntk) of grid k -> L(e), P(e+1).  Lanes of a warp
+// stride over the lines when stride > 1 (lane 0 stores the warp sum).
+template <bool F64>
+__device__ void gather_edge(const NearStore<F64> &st, int k, int e, const typename NearStore<F64>::Real *vb,
+                            int cap, void *scr, int lane, int stride) {
   using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
-  const int ntk = nt_k(k);
+  const int ntk = nt_k(k), sh = 11 - k;
+  const bool hasL = e >= 1, hasP = e <= ntk - 1;
+  const int wl = 2 * ((e + 1) / 2) + 2, wp = 2 * ((e + 2) / 2) + 2; // walk ends of e, e+1 in bins
   Acc<F64> aL, aP;
   aL.init();
   aP.init();
-  const bool hasL = e >= 1, hasP = e <= ntk - 1;
-  { // centre lines, left walk: UU in [(e+1)hk, walk_hi(e)) -> L(e); [(e+2)hk, walk_hi(e+1)) -> P(e+1)
-    const double xl0 = (double)(e + 1) * hk, xp0 = (double)(e + 2) * hk;
-    const double xlh = walk_hi(e, hk), xph = walk_hi(e + 1, hk);
-    const double xlo = hasL ? xl0 : xp0;
-    const double xhi = hasL && hasP ? fmax(xlh, xph) : (hasL ? xlh : xph);
-    const int q0 = st.lb_uu(curL, xlo);
-    curL = q0;
-    const int q1 = st.lb_uu(q0, xhi);
-    for (int q = q0 + lane; q < q1; q += stride) {
-      const double UU = st.uu[q];
-      const bool tl = hasL && UU >= xl0 && UU < xlh;
-      const bool tp = hasP && UU >= xp0 && UU < xph;
-      if (!(tl || tp)) continue;
-      const Real f = st.template evalc<CHI>(q, UU - (double)e * hk);
-      if (tl) aL.add(f);
-      if (tp) aP.add(f);
+  Real f[GB];
+  bool tl[GB], tp[GB];
+  auto flush = [&]() {
+#pragma unroll
+    for (int j = 0; j < GB; ++j) {
+      if (tl[j]) aL.add(f[j]);
+      if (tp[j]) aP.add(f[j]);
+    }
+  };
+  { // left walk: bins e+1 .. e+3
+    const int q0 = st.lbL(k, e + 1), q1 = st.lbL(k, e + 4);
+    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        const int n = q < q1 ? st.n11[q] >> sh : -1;
+        tl[j] = hasL && n >= e + 1 && n < wl;
+        tp[j] = hasP && n >= e + 2 && n < wp;
+        f[j] = (tl[j] || tp[j]) ? vb[(size_t)(n - 1 - e) * cap + q] : (Real)0;
+      }
+      flush();
     }
   }
-  { // centre lines, right walk: V = 10 - UU; cell j counted r = ntk+1-j from the right
+  { // right walk: V bins ntk-e+1 .. ntk-e+3
     const int rL = ntk + 1 - e, rP = ntk - e;
-    const double yl0 = (double)(rL + 1) * hk, ylh = walk_hi(rL, hk);
-    const double yp0 = (double)(rP + 1) * hk, yph = walk_hi(rP, hk);
-    const double ylo = hasP ? yp0 : yl0;
-    const double yhi = hasL && hasP ? fmax(ylh, yph) : (hasL ? ylh : yph);
-    const int q0 = st.lb_v(curR, yhi);
-    curR = q0;
-    const int q1 = st.lb_v(q0, ylo);
-    for (int q = q0 + lane; q < q1; q += stride) {
-      const double V = DELTA_WV - st.uu[q];
-      const bool tl = hasL && V >= yl0 && V < ylh;
-      const bool tp = hasP && V >= yp0 && V < yph;
-      if (!(tl || tp)) continue;
-      const Real f = st.template evalc<CHI>(q, V - (double)rP * hk);
-      if (tl) aL.add(f);
-      if (tp) aP.add(f);
+    const int wrl = 2 * ((rL + 1) / 2) + 2, wrp = 2 * ((rP + 1) / 2) + 2;
+    const int q0 = st.lbV(k, ntk - e + 4), q1 = st.lbV(k, ntk - e + 1);
+    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        const int nv = q < q1 ? st.nv11[q] >> sh : -1;
+        tl[j] = hasL && nv >= rL + 1 && nv < wrl;
+        tp[j] = hasP && nv >= rP + 1 && nv < wrp;
+        f[j] = (tl[j] || tp[j]) ? vb[(size_t)(5 + e - (ntk - nv + 1)) * cap + q] : (Real)0;
+      }
+      flush();
     }
   }
-  if (e <= 2) { // near-left lines (D = -UU < 1): cells 1, 2 of grid k (leftLBL labels 20-28, 121-129)
+  if (e <= 2) { // near-left lines with D < H_{k-1}
     const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
-    for (int q = q0 + lane; q < st.c0; q += stride) {
-      const double UU = st.uu[q], D = -UU;
-      const bool own = D >= hk; // H_k <= D < H_{k-1}: cells 1 and 2 of this grid
-      double X;
-      bool tl = false, tp = false;
-      if (e == 0) { tp = own; X = UU; }
-      else if (e == 1) { tl = own; tp = true; X = UU - hk; }
-      else { tl = true; X = UU - hk1; }
-      if (!(tl || tp)) continue;
-      const Real f = st.template evalc<CHI>(q, X);
-      if (tl) aL.add(f);
-      if (tp) aP.add(f);
+    for (int qb = q0 + lane; qb < st.c0; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        const bool in = q < st.c0;
+        const bool own = in && -st.uu[q] >= hk;
+        tl[j] = in && ((e == 1 && own) || e == 2);
+        tp[j] = in && ((e == 0 && own) || e == 1);
+        f[j] = (tl[j] || tp[j]) ? vb[(size_t)e * cap + q] : (Real)0;
+      }
+      flush();
     }
   }
-  if (e >= ntk - 2) { // near-right lines (U < 1): cells ntk, ntk-1 (rightLBL labels 60-69, 131-139)
+  if (e >= ntk - 2) { // near-right lines with U < H_{k-1}
     const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
-    for (int q = st.c1 + lane; q < q1; q += stride) {
-      const double U = st.uu[q] - DELTA_WV;
-      const bool own = U >= hk;
-      double X;
-      bool tl = false, tp = false;
-      if (e == ntk) { tl = own; X = U; }
-      else if (e == ntk - 1) { tp = own; tl = true; X = U + hk; }
-      else { tp = true; X = U + hk1; }
-      if (!(tl || tp)) continue;
-      const Real f = st.template evalc<CHI>(q, X);
-      if (tl) aL.add(f);
-      if (tp) aP.add(f);
+    for (int qb = st.c1 + lane; qb < q1; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        const bool in = q < q1;
+        const bool own = in && (st.uu[q] - DELTA_WV) >= hk;
+        tl[j] = in && ((e == ntk && own) || e == ntk - 1);
+        tp[j] = in && ((e == ntk - 1 && own) || e == ntk - 2);
+        f[j] = (tl[j] || tp[j]) ? vb[(size_t)(ntk - e) * cap + q] : (Real)0;
+      }
+      flush();
     }
   }
   const bool coop = stride > 1;
@@ -600,115 +840,128 @@ __device__ void fine_edge_site(const NearStore<F64> &st, int k, int e, int &curL
   }
 }
 
-// One mid site m of grid k (1..9): M(m).
-template <bool F64, int CHI>
-__device__ void fine_mid_site(const NearStore<F64> &st, int k, int m, int &curL, int &curR, void *scr,
-                              int lane, int stride) {
+// Site half: mid m (1..ntk) of grid k -> M(m).
+template <bool F64>
+__device__ void gather_mid(const NearStore<F64> &st, int k, int m, const typename NearStore<F64>::Real *vb,
+                           int cap, void *scr, int lane, int stride) {
   using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
-  const double hn = h_k(k + 1); // H_{k+1}; grid 9 writes H+H, the same number
-  const int ntk = nt_k(k);
+  const int ntk = nt_k(k), sh = 11 - k;
   Acc<F64> aM;
   aM.init();
-  {
-    const double x0 = (double)(m + 1) * hk, xh = walk_hi(m, hk);
-    const int q0 = st.lb_uu(curL, x0);
-    curL = q0;
-    const int q1 = st.lb_uu(q0, xh);
-    for (int q = q0 + lane; q < q1; q += stride)
-      aM.add(st.template evalc<CHI>(q, (st.uu[q] - (double)m * hk) + hn));
+  Real f[GB];
+  bool on[GB];
+  auto flush = [&]() {
+#pragma unroll
+    for (int j = 0; j < GB; ++j)
+      if (on[j]) aM.add(f[j]);
+  };
+  { // left walk: bins m+1, m+2
+    const int wm = 2 * ((m + 1) / 2) + 2;
+    const int q0 = st.lbL(k, m + 1), q1 = st.lbL(k, m + 3);
+    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        const int n = q < q1 ? st.n11[q] >> sh : -1;
+        on[j] = n >= m + 1 && n < wm;
+        f[j] = on[j] ? vb[(size_t)(3 + n - 1 - m) * cap + q] : (Real)0;
+      }
+      flush();
+    }
   }
-  {
-    const int r = ntk + 1 - m;
-    const double y0 = (double)(r + 1) * hk, yh = walk_hi(r, hk);
-    const int q0 = st.lb_v(curR, yh);
-    curR = q0;
-    const int q1 = st.lb_v(q0, y0);
-    for (int q = q0 + lane; q < q1; q += stride)
-      aM.add(st.template evalc<CHI>(q, ((DELTA_WV - st.uu[q]) - (double)r * hk) + hn));
+  { // right walk: V bins r+1, r+2 with r = ntk+1-m
+    const int r = ntk + 1 - m, wr = 2 * ((r + 1) / 2) + 2;
+    const int q0 = st.lbV(k, r + 3), q1 = st.lbV(k, r + 1);
+    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        const int nv = q < q1 ? st.nv11[q] >> sh : -1;
+        on[j] = nv >= r + 1 && nv < wr;
+        f[j] = on[j] ? vb[(size_t)(8 + m - (ntk + 2 - nv)) * cap + q] : (Real)0;
+      }
+      flush();
+    }
   }
   if (m <= 2) {
     const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
-    for (int q = q0 + lane; q < st.c0; q += stride) {
-      const double UU = st.uu[q], D = -UU;
-      if (m == 1) {
-        if (D >= hk) aM.add(st.template evalc<CHI>(q, UU - hn));
-      } else {
-        aM.add(st.template evalc<CHI>(q, (UU - hk) - hn));
+    for (int qb = q0 + lane; qb < st.c0; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        on[j] = q < st.c0 && (m == 2 || -st.uu[q] >= hk);
+        f[j] = on[j] ? vb[(size_t)(2 + m) * cap + q] : (Real)0;
       }
+      flush();
     }
   }
   if (m >= ntk - 1) {
     const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
-    for (int q = st.c1 + lane; q < q1; q += stride) {
-      const double U = st.uu[q] - DELTA_WV;
-      if (m == ntk) {
-        if (U >= hk) aM.add(st.template evalc<CHI>(q, U + hn));
-      } else {
-        aM.add(st.template evalc<CHI>(q, (U + hk) + hn));
+    for (int qb = st.c1 + lane; qb < q1; qb += GB * stride) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j * stride;
+        on[j] = q < q1 && (m == ntk - 1 || (st.uu[q] - DELTA_WV) >= hk);
+        f[j] = on[j] ? vb[(size_t)(3 + ntk - m) * cap + q] : (Real)0;
       }
+      flush();
     }
   }
   const double vM = coop_sum(aM.value(), stride > 1);
-  if (lane == 0) {
-    Real *o = (Real *)scr;
-    o[SCR_FINE_M + base_k(k) - NT0 + m - 1] = (Real)vM;
-  }
+  if (lane == 0) ((Real *)scr)[SCR_FINE_M + base_k(k) - NT0 + m - 1] = (Real)vM;
 }
 
-// One finest point i (2..NT): direct contributions to RK(i).
-template <bool F64, int CHI>
-__device__ void fine_point_site(const NearStore<F64> &st, int i, int &curL, int &curR, void *scr) {
+// Site half: finest point i (2..NT) -> RK(i).
+template <bool F64>
+__device__ void gather_point(const NearStore<F64> &st, int i, const typename NearStore<F64>::Real *vb, int cap,
+                             void *scr) {
   using Real = typename NearStore<F64>::Real;
-  const double H = HSTEP, H9 = h_k(9);
-  const double xi = (double)(i - 1) * H;
+  const double H9 = h_k(9);
   Acc<F64> a;
   a.init();
-  // centre lines, left fine loop (LineGridCalc.f90:332-339): UU in [(i-1)H, (4q+8)H), q = (i-2)/4
-  const double xh = (double)(4 * ((i - 2) / 4) + 8) * H;
-  const int qa = st.lb_uu(curL, xi);
-  curL = qa;
-  for (int q = qa; q < st.c1; ++q) {
-    const double UU = st.uu[q];
-    if (UU >= xh) break;
-    a.add(st.template evalc<CHI>(q, UU - xi));
+  Real f[GB];
+  bool on[GB];
+  auto flush = [&]() {
+#pragma unroll
+    for (int j = 0; j < GB; ++j)
+      if (on[j]) a.add(f[j]);
+  };
+  const int qa = st.lbL(11, i - 1);
+  { // left fine loop: UU in [(i-1) H, (4 floor((i-2)/4) + 8) H)
+    const int qe = st.lbL(11, 4 * ((i - 2) / 4) + 8);
+    for (int qb = qa; qb < qe; qb += GB) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j;
+        on[j] = q < qe;
+        f[j] = on[j] ? vb[(size_t)(st.n11[q] + 1 - i) * cap + q] : (Real)0;
+      }
+      flush();
+    }
   }
-  // centre lines, right fine loop (LineGridCalc.f90:485-490): UU < (i-1)H and V < H9 ((NT-i)/4 + 2)
-  const double yv = (double)((NT - i) / 4 + 2) * H9;
-  const int qb = st.lb_v(curR, yv);
-  curR = qb;
-  for (int q = qb; q < qa; ++q) a.add(st.template evalc<CHI>(q, st.uu[q] - xi));
-  if (i <= 5) { // near-left lines with D < H9 (leftLBL label 29)
+  { // right fine loop: UU < (i-1) H and V < (floor((NT-i)/4) + 2) H9
+    const int qb0 = st.lbV(9, (NT - i) / 4 + 2);
+    for (int qb = qb0; qb < qa; qb += GB) {
+#pragma unroll
+      for (int j = 0; j < GB; ++j) {
+        const int q = qb + j;
+        on[j] = q < qa;
+        f[j] = on[j] ? vb[(size_t)(7 + i - st.n11[q] - 2) * cap + q] : (Real)0;
+      }
+      flush();
+    }
+  }
+  if (i <= 5) {
     const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -H9; });
-    for (int q = q0; q < st.c0; ++q) {
-      const double UU = st.uu[q];
-      const double X = i == 2 ? UU - H : (i == 3 ? (UU - H) - H : (i == 4 ? (UU + H) - H9 : UU - H9));
-      a.add(st.template evalc<CHI>(q, X));
-    }
+    for (int q = q0; q < st.c0; ++q) a.add(vb[(size_t)(i - 2) * cap + q]);
   }
-  if (i >= NT - 3) { // near-right lines with U < H9 (rightLBL label 69)
+  if (i >= NT - 3) {
     const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= H9; });
-    for (int q = st.c1; q < q1; ++q) {
-      const double U = st.uu[q] - DELTA_WV;
-      const double X = i == NT ? U : (i == NT - 1 ? U + H : (i == NT - 2 ? (U + H) + H : (U + H9) - H));
-      a.add(st.template evalc<CHI>(q, X));
-    }
+    for (int q = st.c1; q < q1; ++q) a.add(vb[(size_t)(NT - i) * cap + q]);
   }
-  Real *o = (Real *)scr;
-  o[SCR_RK + i - 2] = (Real)a.value();
+  ((Real *)scr)[SCR_RK + i - 2] = (Real)a.value();
 }
-
-// site families of the fine phase: grid k edges (k=1..9), grid k mids, finest points
-__device__ __forceinline__ void family_of(int f, int &kind, int &k, int &n) {
-  if (f < 9) { kind = 0; k = f + 1; n = nt_k(k) + 1; }
-  else if (f < 18) { kind = 1; k = f - 8; n = nt_k(k); }
-  else { kind = 2; k = 0; n = NT - 1; }
-}
-
-constexpr int FINE_RUN = 8;
-constexpr int FINE_THREADS = 512;
-constexpr int COOP_K = 5; // grids 1..COOP_K: warp per site
-__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 
 __device__ __forceinline__ int block_excl_scan(int v, int &total) {
   __shared__ int ws[32];
@@ -737,11 +990,12 @@ __device__ __forceinline__ int block_excl_scan(int v, int &total) {
   return r;
 }
 
+// One (level, subinterval) unit: near lines staged, grid 0 reduced, then the
+// ten passes of the fine grids.
 template <bool F64, int CHI>
-__global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FineParams p) {
+__device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem) {
   using Real = typename NearStore<F64>::Real;
-  extern __shared__ __align__(16) unsigned char fine_smem[];
-  const int u = p.unit0 + blockIdx.x;
+  const int u = p.unit0 + ub;
   const int l = u / p.win.n_sub, sub = u - l * p.win.n_sub;
   const double *snu = p.snu + (size_t)l * p.n_lines;
   const int *sidx = p.sidx + (size_t)l * p.n_lines;
@@ -754,16 +1008,14 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
   if (threadIdx.x < 4) sb[threadIdx.x] = near_bound(snu, p.n_lines, s, se, threadIdx.x);
   if (threadIdx.x < 2) s_counts[threadIdx.x] = 0;
   __syncthreads();
-  const int64_t a = sb[0], c0 = sb[1], c1 = sb[2], b = sb[3];
+  const int64_t a = sb[0], b = sb[3];
   const int cnt = (int)(b - a);
-  long long *pc = p.phase_clock ? p.phase_clock + (size_t)blockIdx.x * 10 : nullptr;
-  __shared__ long long s_fam[3];
-  if (threadIdx.x < 3) s_fam[threadIdx.x] = 0;
+  long long *pc = p.phase_clock ? p.phase_clock + (size_t)ub * 10 : nullptr;
   if (pc && threadIdx.x == 0) { pc[0] = clock64(); pc[5] = cnt; }
   // staging area: shared memory, or this block's slice of the global staging buffer
-  const int cap = cnt <= p.smem_cap ? p.smem_cap : p.gstage_cap;
-  unsigned char *base = cnt <= p.smem_cap ? fine_smem
-                                           : (unsigned char *)p.gstage + (size_t)blockIdx.x * p.gstage_bytes;
+  const bool staged_smem = cnt <= p.smem_cap;
+  const int cap = staged_smem ? p.smem_cap : p.gstage_cap;
+  unsigned char *base = staged_smem ? fine_smem : (unsigned char *)p.gstage + (size_t)blockIdx.x * p.gstage_bytes;
   NearStore<F64> st;
   st.uu = (double *)base;
   st.qx = st.uu + cap;
@@ -771,6 +1023,9 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
   st.lorA = (Real *)(st.vy + cap);
   st.g2 = st.lorA + cap;
   st.hum = st.g2 + cap;
+  short *n11 = (short *)(st.hum + cap), *nv11 = n11 + cap;
+  st.n11 = n11;
+  st.nv11 = nv11;
   st.lv = p.lv[l];
   st.sqrt14 = p.c.sqrt14;
   const double sscale = F64 ? 1.0 : p.sscale;
@@ -789,6 +1044,9 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
     const int pos = m_total + block_excl_scan(keep, tot);
     if (keep && pos < cap) {
       st.uu[pos] = UU;
+      // bins of the centre lines (UU in [0, 10)): at most 20480
+      n11[pos] = cls == 1 ? (short)(int)floor(UU * 2048.0) : (short)0;
+      nv11[pos] = cls == 1 ? (short)(int)floor((DELTA_WV - UU) * 2048.0) : (short)0;
       if (p.shape == 0) {
         const ShapeP<Real> sp = shape_params<Real>(gen[li], p.c, sscale);
         st.qx[pos] = sp.qx;
@@ -810,17 +1068,18 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
   st.m = min(m_total, cap);
   st.c0 = s_counts[0];
   st.c1 = s_counts[1];
-  Real *scr = (Real *)p.scratch + (size_t)blockIdx.x * SCR_STRIDE;
+  Real *scr = (Real *)p.scratch + (size_t)ub * SCR_STRIDE;
   if (m_total > cap) { // cannot happen when the host sized the staging area
     if (threadIdx.x == 0) atomicMax(p.err, 14);
+    __syncthreads();
     return;
   }
   // bucket table of the centre lines: bucket b's entry is the first line
   // whose bucket is >= b; written by the line that opens the bucket range
   __shared__ int s_first[NBUCKET + 1];
   for (int q = st.c0 + threadIdx.x; q <= st.c1; q += blockDim.x) {
-    const int bq = q < st.c1 ? min((int)floor(st.uu[q] * BUCKETS_PER_CM), NBUCKET) : NBUCKET + 1;
-    const int bp = q > st.c0 ? min((int)floor(st.uu[q - 1] * BUCKETS_PER_CM), NBUCKET) : -1;
+    const int bq = q < st.c1 ? min(st.n11[q] >> 3, NBUCKET) : NBUCKET + 1;
+    const int bp = q > st.c0 ? min(st.n11[q - 1] >> 3, NBUCKET) : -1;
     for (int bb = bp + 1; bb <= min(bq, NBUCKET); ++bb) s_first[bb] = q;
   }
   __syncthreads();
@@ -847,65 +1106,70 @@ __global__ void __launch_bounds__(FINE_THREADS, F64 ? 1 : 2) fine_kernel(FinePar
     __syncthreads();
     if (threadIdx.x < 31) scr[threadIdx.x] = (Real)g0[threadIdx.x];
   }
-
   __syncthreads();
   if (pc && threadIdx.x == 0) pc[2] = clock64();
-  // grids 1..COOP_K: one warp per site, lanes over the contributing lines
-  {
-    const int lane = threadIdx.x & 31;
-    int curL = st.c0, curR = st.c0;
-    int prev_k = -1, prev_kind = -1;
-    int site = warp_id(), total = 0;
-    for (int kk = 1; kk <= COOP_K; ++kk) total += 2 * nt_k(kk) + 1;
-    for (; site < total; site += blockDim.x >> 5) {
-      int kk = 1, rem = site;
-      while (rem >= 2 * nt_k(kk) + 1) { rem -= 2 * nt_k(kk) + 1; ++kk; }
-      const int kind = rem <= nt_k(kk) ? 0 : 1;
-      if (kk != prev_k || kind != prev_kind) { curL = st.c0; curR = st.c0; prev_k = kk; prev_kind = kind; }
-      if (kind == 0) fine_edge_site<F64, CHI>(st, kk, rem, curL, curR, scr, lane, 32);
-      else fine_mid_site<F64, CHI>(st, kk, rem - nt_k(kk), curL, curR, scr, lane, 32);
-    }
-  }
-  if (pc) {
+
+  // slot buffer: in shared memory behind the staged lines when its rows fit
+  // there (units staged in shared memory only), else this block's global slice
+  Real *vb_g = (Real *)p.vbuf + (size_t)blockIdx.x * p.vbuf_stride;
+  Real *vb_s = (Real *)(fine_smem + (size_t)p.smem_cap * (24 + 3 * sizeof(Real) + 4));
+  long long t_line = 0, t_site = 0;
+  for (int k = 1; k <= 10; ++k) {
+    const bool vsm = staged_smem && (k <= 9 ? 10 : NSLOT) <= p.vsm_rows;
+    Real *vb = vsm ? vb_s : vb_g;
+    const int vcap = vsm ? p.smem_cap : p.vbuf_cap;
+    const long long t0 = pc ? clock64() : 0;
+    for (int q = threadIdx.x; q < st.m; q += blockDim.x) line_pass<F64, CHI>(st, q, k, vb, vcap);
     __syncthreads();
-    if (threadIdx.x == 0) pc[3] = clock64();
-  }
-  // grids COOP_K+1..9 and finest points: runs of FINE_RUN consecutive sites per thread
-  int runs_total = 0;
-  for (int f = 0; f < 19; ++f) {
-    int kind, k, n;
-    family_of(f, kind, k, n);
-    if (kind != 2 && k <= COOP_K) continue;
-    runs_total += (n + FINE_RUN - 1) / FINE_RUN;
-  }
-  for (int r = threadIdx.x; r < runs_total; r += blockDim.x) {
-    int f = 0, rbase = 0, kind = 0, k = 0, n = 0;
-    for (; f < 19; ++f) {
-      family_of(f, kind, k, n);
-      if (kind != 2 && k <= COOP_K) continue;
-      const int nr_f = (n + FINE_RUN - 1) / FINE_RUN;
-      if (r < rbase + nr_f) break;
-      rbase += nr_f;
+    const long long t1 = pc ? clock64() : 0;
+    if (k <= COOP_K) {
+      const int lane = threadIdx.x & 31, nsite = 2 * nt_k(k) + 1;
+      for (int site = warp_id(); site < nsite; site += blockDim.x >> 5) {
+        if (site <= nt_k(k)) gather_edge<F64>(st, k, site, vb, vcap, scr, lane, 32);
+        else gather_mid<F64>(st, k, site - nt_k(k), vb, vcap, scr, lane, 32);
+      }
+    } else if (k <= 9) {
+      const int ntk = nt_k(k), nsite = 2 * ntk + 1;
+      for (int site = threadIdx.x; site < nsite; site += blockDim.x) {
+        if (site <= ntk) gather_edge<F64>(st, k, site, vb, vcap, scr, 0, 1);
+        else gather_mid<F64>(st, k, site - ntk, vb, vcap, scr, 0, 1);
+      }
+    } else {
+      for (int i = 2 + threadIdx.x; i <= NT; i += blockDim.x) gather_point<F64>(st, i, vb, vcap, scr);
     }
-    const int first = (r - rbase) * FINE_RUN;
-    const int last = min(first + FINE_RUN, n);
-    int curL = st.c0, curR = st.c0;
-    const long long tr0 = pc ? clock64() : 0;
-    for (int t = first; t < last; ++t) {
-      if (kind == 0) fine_edge_site<F64, CHI>(st, k, t, curL, curR, scr, 0, 1);
-      else if (kind == 1) fine_mid_site<F64, CHI>(st, k, t + 1, curL, curR, scr, 0, 1);
-      else fine_point_site<F64, CHI>(st, t + 2, curL, curR, scr);
-    }
-    if (pc) atomicAdd((unsigned long long *)&s_fam[kind], (unsigned long long)(clock64() - tr0));
-  }
-  if (pc) {
     __syncthreads();
+    if (pc && threadIdx.x == 0) {
+      const long long t2 = clock64();
+      t_line += t1 - t0;
+      t_site += t2 - t1;
+      if (k == COOP_K) pc[3] = t2;
+      if (k == 6) pc[6] = t2;
+      if (k == 9) pc[7] = t2;
+    }
+  }
+  if (pc && threadIdx.x == 0) {
+    pc[4] = clock64();
+    pc[8] = t_line;
+    pc[9] = t_site;
+  }
+}
+
+// Persistent: every block takes units from the work queue until it is empty
+// (units in the given order, most near lines first).
+template <bool F64, int CHI>
+__global__ void __launch_bounds__(FINE_THREADS, 1) fine_kernel(FineParams p) {
+  extern __shared__ __align__(16) unsigned char fine_smem[];
+  __shared__ int s_unit;
+  for (;;) {
     if (threadIdx.x == 0) {
-      pc[4] = clock64();
-      pc[6] = s_fam[0];
-      pc[7] = s_fam[1];
-      pc[8] = s_fam[2];
+      const int t = atomicAdd(p.queue, 1);
+      s_unit = t < p.n_units ? (p.order ? p.order[t] : t) : -1;
     }
+    __syncthreads();
+    const int ub = s_unit;
+    __syncthreads();
+    if (ub < 0) break;
+    fine_unit<F64, CHI>(p, ub, fine_smem);
   }
 }
 
@@ -1249,11 +1513,37 @@ cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t 
 
 template <bool F64, int CHI>
 static cudaError_t fine_launch(const FineParams &p, cudaStream_t st) {
-  const size_t smem = fine_smem_bytes(p.smem_cap, F64);
+  const size_t smem = fine_smem_bytes(p.smem_cap, F64, p.vsm_rows);
   cudaError_t e = cudaFuncSetAttribute(fine_kernel<F64, CHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  fine_kernel<F64, CHI><<<p.n_units, FINE_THREADS, smem, st>>>(p);
+  fine_kernel<F64, CHI><<<p.grid, FINE_THREADS, smem, st>>>(p);
   return cudaGetLastError();
+}
+
+// Shared-memory plan of the fine kernel for `smem_cap` staged lines: the
+// most slot-buffer rows (NSLOT, 10 or 0) that fit beside the staging area,
+// and the resident blocks of the persistent grid.
+template <bool F64, int CHI>
+static cudaError_t fine_occupancy(int smem_cap, int *rows, int *blocks) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI>);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, optin = 0;
+  if ((e = cudaGetDevice(&dev))) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+  const size_t room = (size_t)optin - fa.sharedSizeBytes;
+  *rows = 0;
+  for (int r : {NSLOT, 10})
+    if (fine_smem_bytes(smem_cap, F64, r) <= room) { *rows = r; break; }
+  const size_t smem = fine_smem_bytes(smem_cap, F64, *rows);
+  if ((e = cudaFuncSetAttribute(fine_kernel<F64, CHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+    return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fine_kernel<F64, CHI>, FINE_THREADS, smem)))
+    return e;
+  *blocks = (per_sm < 1 ? 1 : per_sm) * sms;
+  return cudaSuccess;
 }
 
 template <bool F64>
@@ -1266,7 +1556,26 @@ static cudaError_t fine_dispatch(const FineParams &p, int chi, cudaStream_t st) 
   }
 }
 
-size_t fine_smem_bytes(int cap, bool f64) { return (size_t)cap * (24 + 3 * (f64 ? 8 : 4)); }
+template <bool F64>
+static cudaError_t fine_occ_dispatch(int chi, int smem_cap, int *rows, int *blocks) {
+  switch (chi) {
+  case CHI_TONKOV: return fine_occupancy<F64, CHI_TONKOV>(smem_cap, rows, blocks);
+  case CHI_POLLACK: return fine_occupancy<F64, CHI_POLLACK>(smem_cap, rows, blocks);
+  case CHI_PERRIN: return fine_occupancy<F64, CHI_PERRIN>(smem_cap, rows, blocks);
+  default: return fine_occupancy<F64, CHI_NONE>(smem_cap, rows, blocks);
+  }
+}
+
+size_t fine_smem_bytes(int cap, bool f64, int vsm_rows) {
+  const size_t r = f64 ? 8 : 4;
+  return (size_t)cap * (24 + 3 * r + 4 + (size_t)vsm_rows * r);
+}
+size_t fine_vbuf_elems(int cap) { return (size_t)NSLOT * cap; }
+
+cudaError_t fine_plan(int precision, int chi, int smem_cap, int *vsm_rows, int *blocks) {
+  return precision == 0 ? fine_occ_dispatch<true>(chi, smem_cap, vsm_rows, blocks)
+                        : fine_occ_dispatch<false>(chi, smem_cap, vsm_rows, blocks);
+}
 
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st) {
   if (p.n_units == 0) return cudaSuccess;

@@ -67,6 +67,10 @@ struct FarParams {
   double *out;                   // [Lc][C][NFAR]
 };
 
+// Rows of the fine kernel's slot buffer (values per staged line; the
+// finest-point pass uses 15).
+constexpr int NSLOT = 15;
+
 struct FineParams {
   const double *snu;
   const int *sidx;
@@ -87,6 +91,13 @@ struct FineParams {
   size_t gstage_bytes;           // bytes per block in gstage
   int *err;
   long long *phase_clock;        // optional [n_units][10] clock64 marks (diagnostics)
+  int *queue;                    // work-queue head (zero before the launch)
+  const int *order;              // optional processing order of the units
+  void *vbuf;                    // per-block slot buffers in global memory
+  size_t vbuf_stride;            // elements per block
+  int vbuf_cap;                  // lines per slot row in vbuf
+  int grid;                      // persistent blocks
+  int vsm_rows;                  // slot-buffer rows held in shared memory (0, 10 or NSLOT)
 };
 
 struct CascadeParams {
@@ -182,7 +193,12 @@ cudaError_t launch_sort(const SortParams &p, cudaStream_t st);
 cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t st);
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st);
 cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st);
-size_t fine_smem_bytes(int cap, bool f64);
+// dynamic shared memory of the fine kernel: `cap` staged lines and
+// `vsm_rows` slot-buffer rows of `cap` values
+size_t fine_smem_bytes(int cap, bool f64, int vsm_rows = 0);
+size_t fine_vbuf_elems(int cap);
+// slot-buffer rows that fit in shared memory and the persistent grid size
+cudaError_t fine_plan(int precision, int chi, int smem_cap, int *vsm_rows, int *blocks);
 cudaError_t fma_peak(bool f64, double *flops_per_s);
 cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st);
 cudaError_t launch_count(const CountParams &p, cudaStream_t st);

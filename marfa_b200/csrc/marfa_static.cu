@@ -55,7 +55,8 @@ constexpr size_t TIPS_MAX = 128 * 1024;                       // doubles of the 
 constexpr size_t OFF_FAR = al(OFF_TIPS + TIPS_MAX * 8);
 constexpr size_t OFF_SCR = al(OFF_FAR + (size_t)MAXC * NFAR * 8);
 constexpr size_t OFF_GST = al(OFF_SCR + (size_t)SCR_STRIDE * 8);
-constexpr size_t OFF_REC = al(OFF_GST + (size_t)GSTAGE_LINES * 48);
+constexpr size_t OFF_VB = al(OFF_GST + (size_t)GSTAGE_LINES * 52);
+constexpr size_t OFF_REC = al(OFF_VB + (size_t)NSLOT * GSTAGE_LINES * 8);
 constexpr size_t OFF_SMALL = al(OFF_REC + (size_t)NT * 4);      // tables, level, counters
 constexpr size_t SMALL_BYTES = 4096 + (size_t)MAXC * 20;
 constexpr size_t TOTAL = al(OFF_SMALL + SMALL_BYTES);
@@ -233,6 +234,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
     int sub_chunk0[2];
     int err;
     int near;
+    int queue;
     LevelConst lv;
     double margin;
   };
@@ -246,6 +248,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   hs.sub_chunk0[1] = C;
   hs.err = 0;
   hs.near = 0;
+  hs.queue = 0;
   hs.lv = lv;
   hs.margin = margin;
   Small *d_small = (Small *)small;
@@ -354,6 +357,13 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
     fn.gstage_cap = (near + 255) / 256 * 256;
     fn.gstage_bytes = fine_smem_bytes(fn.gstage_cap, f64);
   }
+  fn.queue = &d_small->queue;
+  fn.order = nullptr;
+  fn.grid = 1;
+  fn.vsm_rows = 0;
+  fn.vbuf = base + OFF_VB;
+  fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
+  fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
   if (m > 0 && !ck(launch_fine(fn, run->precision, chi, st), "fine")) return rc;
   if (m == 0) { // no line in the window: an all-zero scratch slab and zero far sums
     if (!ck(cudaMemsetAsync(base + OFF_SCR, 0, (size_t)SCR_STRIDE * (f64 ? 8 : 4), st), "zero scratch")) return rc;
