@@ -49,8 +49,13 @@ struct marfa_ctx {
   int *d_err = nullptr;
   // grow-only work buffers
   DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
-      b_out, b_out64, b_dump, b_count, b_near, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order;
+      b_out, b_out64, b_dump, b_count, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order;
   std::string err;
+  // pinned staging of the per-call host tables (see Staging)
+  void *pinned = nullptr;
+  size_t pinned_cap = 0;
+  cudaEvent_t pinned_ev = nullptr;
+  bool pinned_pending = false;
   std::vector<cudaEvent_t> events;
   // timing marks of the last compute call: (family, start, stop); family 5
   // is the whole call
@@ -100,6 +105,51 @@ void release(DevBuf &b) {
   b.p = nullptr;
   b.cap = 0;
 }
+
+} // namespace
+
+namespace {
+
+// The host tables of one call (windows, chunks, levels, work order) reach the
+// device through one pinned buffer of the context: a copy from pageable memory
+// would first wait for the stream to drain, so that the host planning of a
+// call could not overlap the kernels of the previous one.  The buffer is
+// rewritten only after the copies of the previous call have completed.
+struct Staging {
+  marfa_ctx *ctx;
+  cudaStream_t st;
+  size_t off = 0;
+  cudaError_t begin(size_t bytes) {
+    cudaError_t e = cudaSuccess;
+    if (ctx->pinned_pending) {
+      if ((e = cudaEventSynchronize(ctx->pinned_ev))) return e;
+      ctx->pinned_pending = false;
+    }
+    if (!ctx->pinned_ev && (e = cudaEventCreateWithFlags(&ctx->pinned_ev, cudaEventDisableTiming))) return e;
+    if (bytes > ctx->pinned_cap) {
+      if (ctx->pinned) cudaFreeHost(ctx->pinned);
+      ctx->pinned = nullptr;
+      ctx->pinned_cap = 0;
+      if ((e = cudaMallocHost(&ctx->pinned, bytes))) return e;
+      ctx->pinned_cap = bytes;
+    }
+    off = 0;
+    return e;
+  }
+  cudaError_t put(void *dst, const void *src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    char *h = (char *)ctx->pinned + off;
+    std::memcpy(h, src, bytes);
+    off += (bytes + 15) & ~(size_t)15;
+    return cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, st);
+  }
+  cudaError_t end() {
+    cudaError_t e = cudaEventRecord(ctx->pinned_ev, st);
+    if (e == cudaSuccess) ctx->pinned_pending = true;
+    return e;
+  }
+  static size_t room(size_t bytes) { return (bytes + 15) & ~(size_t)15; }
+};
 
 // Constants of Constants.f90 evaluated in double.
 Consts make_consts() {
@@ -334,16 +384,6 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   int64_t *d_cb = (int64_t *)cb;
   int64_t *d_ce = d_cb + std::max(C, 1);
   int *d_cs = (int *)(d_ce + std::max(C, 1));
-  CK(cudaMemcpyAsync(d_s, pl.s.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
-  CK(cudaMemcpyAsync(d_e, pl.e.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
-  CK(cudaMemcpyAsync(d_lo, pl.lo.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
-  CK(cudaMemcpyAsync(d_hi, pl.hi.data(), nsub * 8, cudaMemcpyHostToDevice, st), "h2d windows");
-  CK(cudaMemcpyAsync(d_sc0, pl.sub_chunk0.data(), (nsub + 1) * 4, cudaMemcpyHostToDevice, st), "h2d windows");
-  if (C > 0) {
-    CK(cudaMemcpyAsync(d_cb, pl.chunk_begin.data(), C * 8, cudaMemcpyHostToDevice, st), "h2d chunks");
-    CK(cudaMemcpyAsync(d_ce, pl.chunk_end.data(), C * 8, cudaMemcpyHostToDevice, st), "h2d chunks");
-    CK(cudaMemcpyAsync(d_cs, pl.chunk_sub.data(), C * 4, cudaMemcpyHostToDevice, st), "h2d chunks");
-  }
   std::vector<double> margin(n_levels);
   for (int l = 0; l < n_levels; ++l) {
     const double a = ctx->dmin * P[l], b = ctx->dmax * P[l];
@@ -351,8 +391,51 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   }
   LevelConst *d_lv = (LevelConst *)ctx->b_lv.p;
   double *d_margin = (double *)ctx->b_margin.p;
-  CK(cudaMemcpyAsync(d_lv, lv.data(), n_levels * sizeof(LevelConst), cudaMemcpyHostToDevice, st), "h2d levels");
-  CK(cudaMemcpyAsync(d_margin, margin.data(), n_levels * 8, cudaMemcpyHostToDevice, st), "h2d margin");
+
+  // Near-line bound of every unit, from the unshifted centres: a near line
+  // has s - 1 < nu' < s + 11 (the bounds of fine_kernel) and nu' = nu + delta
+  // P with delta in [dmin, dmax], so nu lies in (s - 1 - dmax P, s + 11 -
+  // dmin P).  The bound sizes the fine kernel's staging and orders its work
+  // queue (most lines first) before anything is launched, so that no call
+  // waits for the device in the middle of its launches.
+  std::vector<int> nbound((size_t)n_levels * nsub), order_all((size_t)n_levels * nsub);
+  for (int l = 0; l < n_levels; ++l)
+    for (int isub = 0; isub < nsub; ++isub) {
+      const double lo = pl.s[isub] - 1.0 - std::max(ctx->dmax, 0.0) * P[l] - 1e-6;
+      const double hi = pl.s[isub] + DELTA_WV + 1.0 - std::min(ctx->dmin, 0.0) * P[l] + 1e-6;
+      const auto a0 = std::lower_bound(ctx->nu.begin(), ctx->nu.end(), lo);
+      const auto b0 = std::upper_bound(a0, ctx->nu.end(), hi);
+      nbound[(size_t)l * nsub + isub] = (int)(b0 - a0);
+    }
+  for (int l0 = 0; l0 < n_levels; l0 += Lc) {
+    const int base = l0 * nsub, units = std::min(Lc, n_levels - l0) * nsub;
+    for (int u0 = 0; u0 < units; u0 += UB) {
+      const int nu_ = std::min(UB, units - u0);
+      int *o_ = order_all.data() + base + u0;
+      for (int i = 0; i < nu_; ++i) o_[i] = i;
+      std::stable_sort(o_, o_ + nu_, [&](int x, int y) { return nbound[base + u0 + x] > nbound[base + u0 + y]; });
+    }
+  }
+  CK(ensure(ctx->b_order, order_all.size() * 4), "alloc order");
+
+  Staging sg{ctx, st};
+  const size_t stage_bytes = 4 * Staging::room((size_t)nsub * 8) + Staging::room((size_t)(nsub + 1) * 4) +
+                             2 * Staging::room((size_t)C * 8) + Staging::room((size_t)C * 4) +
+                             Staging::room((size_t)n_levels * sizeof(LevelConst)) +
+                             Staging::room((size_t)n_levels * 8) + Staging::room(order_all.size() * 4);
+  CK(sg.begin(stage_bytes), "pinned staging");
+  CK(sg.put(d_s, pl.s.data(), nsub * 8), "h2d windows");
+  CK(sg.put(d_e, pl.e.data(), nsub * 8), "h2d windows");
+  CK(sg.put(d_lo, pl.lo.data(), nsub * 8), "h2d windows");
+  CK(sg.put(d_hi, pl.hi.data(), nsub * 8), "h2d windows");
+  CK(sg.put(d_sc0, pl.sub_chunk0.data(), (nsub + 1) * 4), "h2d windows");
+  CK(sg.put(d_cb, pl.chunk_begin.data(), (size_t)C * 8), "h2d chunks");
+  CK(sg.put(d_ce, pl.chunk_end.data(), (size_t)C * 8), "h2d chunks");
+  CK(sg.put(d_cs, pl.chunk_sub.data(), (size_t)C * 4), "h2d chunks");
+  CK(sg.put(d_lv, lv.data(), n_levels * sizeof(LevelConst)), "h2d levels");
+  CK(sg.put(d_margin, margin.data(), n_levels * 8), "h2d margin");
+  CK(sg.put(ctx->b_order.p, order_all.data(), order_all.size() * 4), "h2d order");
+  CK(sg.end(), "staging event");
   CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st), "memset err");
 
   WindowTable win{d_s, d_e, d_lo, d_hi, nsub};
@@ -476,15 +559,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * 10 * 8, st), "memset clock");
       fn.phase_clock = (long long *)ctx->b_count.p;
     }
-    fn.unit0 = 0;
-    fn.n_units = units;
-    CK(ensure(ctx->b_near, (size_t)units * 4), "alloc near counts");
-    CK(launch_near_count(fn, (int *)ctx->b_near.p, st), "near count kernel");
-    ctx->launches += 1;
-    std::vector<int> ncount(units);
-    CK(cudaMemcpyAsync(ncount.data(), ctx->b_near.p, (size_t)units * 4, cudaMemcpyDeviceToHost, st), "d2h near");
-    CK(cudaStreamSynchronize(st), "sync near");
-    const int max_near = units ? *std::max_element(ncount.begin(), ncount.end()) : 0;
+    const int max_near = units ? *std::max_element(nbound.begin() + (size_t)l0 * nsub,
+                                                   nbound.begin() + (size_t)l0 * nsub + units) : 0;
     // staged lines per block in shared memory; units with more near lines
     // stage in a global slice of their block
     const int smem_max = f64 ? 4096 : 2688;
@@ -504,23 +580,12 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.vbuf = ctx->b_vbuf.p;
     CK(ensure(ctx->b_queue, 256), "alloc queue");
     fn.queue = (int *)ctx->b_queue.p;
-    // work order of every batch: most near lines first
     const int UBc = UB;
-    std::vector<int> order(units);
-    for (int u0 = 0; u0 < units; u0 += UBc) {
-      const int nu_ = std::min(UBc, units - u0);
-      for (int i = 0; i < nu_; ++i) order[u0 + i] = i;
-      std::stable_sort(order.begin() + u0, order.begin() + u0 + nu_,
-                       [&](int x, int y) { return ncount[u0 + x] > ncount[u0 + y]; });
-    }
-    CK(ensure(ctx->b_order, (size_t)units * 4), "alloc order");
-    CK(cudaMemcpyAsync(ctx->b_order.p, order.data(), (size_t)units * 4, cudaMemcpyHostToDevice, st), "h2d order");
-    CK(cudaStreamSynchronize(st), "sync order"); // `order` is a host temporary
     for (int u0 = 0; u0 < units; u0 += UBc) {
       const int nu_ = std::min(UBc, units - u0);
       fn.unit0 = u0;
       fn.n_units = nu_;
-      fn.order = (const int *)ctx->b_order.p + u0;
+      fn.order = (const int *)ctx->b_order.p + (size_t)l0 * nsub + u0;
       fn.grid = std::min(resident, nu_);
       cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
       if (f0) cudaEventRecord(f0, st);
@@ -765,9 +830,11 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
     if (p) cudaFree(p);
   DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
                   &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
-                  &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_near, &ctx->b_gstage, &ctx->b_aux,
+                  &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_gstage, &ctx->b_aux,
                   &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order};
   for (DevBuf *b : bs) release(*b);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
