@@ -37,8 +37,9 @@ extern "C" {
 #define MARFA_E_TEMPERATURE 11  /* level temperature outside the TIPS table          */
 #define MARFA_E_UNSORTED 12     /* line list not sorted by wavenumber                */
 #define MARFA_E_ISOTOPE 13      /* jointMolIso/100 outside the WISO/TIPS tables      */
-#define MARFA_E_CAPACITY 15     /* input larger than marfa_compute_record_static's   */
-                                /* fixed storage                                     */
+#define MARFA_E_CAPACITY 15     /* input beyond a fixed capacity: the storage of     */
+                                /* marfa_compute_record_static, or more than 65535   */
+                                /* lines within 1 cm-1 of one subinterval            */
 #define MARFA_E_CUDA 100        /* CUDA runtime error (see marfa_last_error)         */
 #define MARFA_E_NOMEM 101       /* device allocation failed                          */
 #define MARFA_E_NODEVICE 110    /* no CUDA device                                    */

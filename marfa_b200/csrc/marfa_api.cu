@@ -561,6 +561,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     }
     const int max_near = units ? *std::max_element(nbound.begin() + (size_t)l0 * nsub,
                                                    nbound.begin() + (size_t)l0 * nsub + units) : 0;
+    if (max_near > 65535) // line indices of one unit are 16-bit in the fine kernel's bin table
+      return set_err(ctx, MARFA_E_CAPACITY, "%d lines within 1 cm-1 of one subinterval (at most 65535)", max_near);
     // staged lines per block in shared memory; units with more near lines
     // stage in a global slice of their block
     const int smem_max = f64 ? 4096 : 2688;

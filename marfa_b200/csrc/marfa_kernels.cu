@@ -396,8 +396,7 @@ struct Acc<false> {
 // reference schedule lets contribute (inside the line window, within the
 // cutoff, centre lines with UU < 10).  Held in shared memory (or, for very
 // dense line lists, in a global staging area) as structure of arrays.
-constexpr double BUCKETS_PER_CM = 256.0;
-constexpr int NBUCKET = 2560; // buckets over the 10 cm-1 subinterval
+constexpr int NBIN9 = 5120; // grid-9 bins over the 10 cm-1 subinterval
 
 template <bool F64>
 struct NearStore {
@@ -425,26 +424,25 @@ struct NearStore {
     }
     return voigt_core<Real, CHI>(X, qxv, vy[q], lorA[q], g2[q], hum[q], lv.perrin_b1, lv.perrin_b2, sqrt14);
   }
-  // first[b] = first centre line with floor(UU * 2^8) >= b, b = 0 .. NBUCKET
-  const int *first;
+  // first[b] = first centre line with floor(UU * 2^9) >= b, b = 0 .. NBIN9
+  const unsigned short *first;
   // centre lines: floor(UU * 2^11) and floor(V * 2^11), V = fl(10 - UU); the
   // bin of grid k is the value shifted right by 11 - k
   const short *n11, *nv11;
-  // first centre line with UU >= a H_k (bin_k >= a)
+  // first centre line with UU >= a H_k (bin_k >= a); exact for grids 1..9,
+  // the finest bins (k = 11) scan within one grid-9 bin
   __device__ __forceinline__ int lbL(int k, int a) const {
-    int b = k <= 8 ? (a << (8 - k)) : (a >> (k - 8));
-    b = b < 0 ? 0 : (b > NBUCKET ? NBUCKET : b);
-    int q = first[b];
-    const int sh = 11 - k;
-    while (q < c1 && (n11[q] >> sh) < a) ++q;
+    if (k <= 9) return first[min(a << (9 - k), NBIN9)];
+    int q = first[min(a >> 2, NBIN9)];
+    while (q < c1 && n11[q] < a) ++q;
     return q;
   }
-  // first centre line with V < a H_k (V bin_k < a); one bucket of margin
-  // below 10 - a H_k covers the rounding of V
+  // first centre line with V < a H_k (V bin_k < a), k <= 9: those lines have
+  // UU > 10 - a H_k; the scan starts one grid-9 bin earlier, which covers the
+  // rounding of V
   __device__ __forceinline__ int lbV(int k, int a) const {
-    const int t = k <= 8 ? (a << (8 - k)) : ((a + (1 << (k - 8)) - 1) >> (k - 8));
-    int b = NBUCKET - t - 1;
-    b = b < 0 ? 0 : (b > NBUCKET ? NBUCKET : b);
+    int b = NBIN9 - (a << (9 - k)) - 1;
+    b = b < 0 ? 0 : (b > NBIN9 ? NBIN9 : b);
     int q = first[b];
     const int sh = 11 - k;
     while (q < c1 && (nv11[q] >> sh) >= a) ++q;
@@ -752,7 +750,7 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
 
 // The site half reads the slot values of up to GB lines per batch, loads
 // first, sums after, so that the loads of a batch are in flight together.
-constexpr int GB = 4;
+constexpr int GB = 2;
 
 // Site half: edge e (0..ntk) of grid k -> L(e), P(e+1).  Lanes of a warp
 // stride over the lines when stride > 1 (lane 0 stores the warp sum).
@@ -1080,13 +1078,13 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     __syncthreads();
     return;
   }
-  // bucket table of the centre lines: bucket b's entry is the first line
-  // whose bucket is >= b; written by the line that opens the bucket range
-  __shared__ int s_first[NBUCKET + 1];
+  // grid-9 bin table of the centre lines: entry b is the first line whose
+  // bin is >= b, written by the line that opens the range of bins
+  __shared__ unsigned short s_first[NBIN9 + 1];
   for (int q = st.c0 + threadIdx.x; q <= st.c1; q += blockDim.x) {
-    const int bq = q < st.c1 ? min(st.n11[q] >> 3, NBUCKET) : NBUCKET + 1;
-    const int bp = q > st.c0 ? min(st.n11[q - 1] >> 3, NBUCKET) : -1;
-    for (int bb = bp + 1; bb <= min(bq, NBUCKET); ++bb) s_first[bb] = q;
+    const int bq = q < st.c1 ? min(st.n11[q] >> 2, NBIN9) : NBIN9 + 1;
+    const int bp = q > st.c0 ? min(st.n11[q - 1] >> 2, NBIN9) : -1;
+    for (int bb = bp + 1; bb <= min(bq, NBIN9); ++bb) s_first[bb] = (unsigned short)q;
   }
   __syncthreads();
   st.first = s_first;
