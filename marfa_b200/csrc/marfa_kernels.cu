@@ -537,7 +537,8 @@ __device__ __forceinline__ double coop_sum(double v, bool coop) {
 // V = fl(10 - UU) and its bin).  Per accumulator the order of summation is:
 // centre lines of the left walk, centre lines of the right walk, near-left
 // lines, near-right lines, each in ascending shifted-centre order.
-constexpr int FINE_THREADS = 512;
+// threads per block: 1024 in the FP32 form (64 registers), 512 in FP64
+__host__ __device__ constexpr int fine_threads(bool f64) { return f64 ? 512 : 1024; }
 constexpr int COOP_K = 3; // grids 1..COOP_K: one warp per site in the site half
 __device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 
@@ -1161,7 +1162,7 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
 // Persistent: every block takes units from the work queue until it is empty
 // (units in the given order, most near lines first).
 template <bool F64, int CHI>
-__global__ void __launch_bounds__(FINE_THREADS, 1) fine_kernel(FineParams p) {
+__global__ void __launch_bounds__(fine_threads(F64), 1) fine_kernel(FineParams p) {
   extern __shared__ __align__(16) unsigned char fine_smem[];
   __shared__ int s_unit;
   for (;;) {
@@ -1520,7 +1521,7 @@ static cudaError_t fine_launch(const FineParams &p, cudaStream_t st) {
   const size_t smem = fine_smem_bytes(p.smem_cap, F64, p.vsm_rows);
   cudaError_t e = cudaFuncSetAttribute(fine_kernel<F64, CHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  fine_kernel<F64, CHI><<<p.grid, FINE_THREADS, smem, st>>>(p);
+  fine_kernel<F64, CHI><<<p.grid, fine_threads(F64), smem, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -1544,7 +1545,7 @@ static cudaError_t fine_occupancy(int smem_cap, int *rows, int *blocks) {
   if ((e = cudaFuncSetAttribute(fine_kernel<F64, CHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
     return e;
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fine_kernel<F64, CHI>, FINE_THREADS, smem)))
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fine_kernel<F64, CHI>, fine_threads(F64), smem)))
     return e;
   *blocks = (per_sm < 1 ? 1 : per_sm) * sms;
   return cudaSuccess;
