@@ -22,7 +22,6 @@ using namespace marfa;
 
 namespace {
 
-constexpr int64_t FAR_CHUNK = 4096; // lines per far-kernel block
 
 struct DevBuf {
   void *p = nullptr;
@@ -31,8 +30,16 @@ struct DevBuf {
 
 } // namespace
 
+// Launch parameters that do not change results (chosen by marfa_autotune).
+struct Tune {
+  int far_chunk = 4096;    // lines per far-kernel block
+  int coop_k = 3;          // fine grids whose sites are summed by one warp each
+  int sparse_lines = 1024; // units with fewer near lines skip untouched sites
+};
+
 struct marfa_ctx {
   int device = 0;
+  Tune tune;
   cudaStream_t stream = nullptr;
   int64_t n_lines = 0;
   std::vector<double> nu;  // host copy of the sorted centres (window scan)
@@ -234,10 +241,11 @@ int make_plan(marfa_ctx *ctx, const marfa_run *run, Plan &pl) {
   pl.sub_chunk0.assign(pl.n_sub + 1, 0);
   for (int isub = 0; isub < pl.n_sub; ++isub) {
     pl.sub_chunk0[isub] = (int)pl.chunk_sub.size();
-    for (int64_t b = pl.lo[isub]; b < pl.hi[isub]; b += FAR_CHUNK) {
+    const int64_t chunk = ctx->tune.far_chunk;
+    for (int64_t b = pl.lo[isub]; b < pl.hi[isub]; b += chunk) {
       pl.chunk_sub.push_back(isub);
       pl.chunk_begin.push_back(b);
-      pl.chunk_end.push_back(std::min(b + FAR_CHUNK, pl.hi[isub]));
+      pl.chunk_end.push_back(std::min(b + chunk, pl.hi[isub]));
     }
   }
   pl.sub_chunk0[pl.n_sub] = (int)pl.chunk_sub.size();
@@ -582,6 +590,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.vbuf = ctx->b_vbuf.p;
     CK(ensure(ctx->b_queue, 256), "alloc queue");
     fn.queue = (int *)ctx->b_queue.p;
+    fn.coop_k = ctx->tune.coop_k;
+    fn.sparse_lines = ctx->tune.sparse_lines;
     const int UBc = UB;
     for (int u0 = 0; u0 < units; u0 += UBc) {
       const int nu_ = std::min(UBc, units - u0);

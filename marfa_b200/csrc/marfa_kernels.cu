@@ -539,7 +539,6 @@ __device__ __forceinline__ double coop_sum(double v, bool coop) {
 // lines, near-right lines, each in ascending shifted-centre order.
 // threads per block: 1024 in the FP32 form (64 registers), 512 in FP64
 __host__ __device__ constexpr int fine_threads(bool f64) { return f64 ? 512 : 1024; }
-constexpr int COOP_K = 3; // grids 1..COOP_K: one warp per site in the site half
 __device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 
 // Line shape of one near line for the fine passes: region 0 inline, Kuntz
@@ -632,11 +631,18 @@ __device__ __forceinline__ double i2d(int n) {
 // The offsets X are exact: UU - e H_k is a multiple of the ulp of UU not
 // larger than UU, and so are its neighbours e -+ 1 built from it.
 template <bool F64, int CHI>
-__device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearStore<F64>::Real *vb, int cap) {
+__device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearStore<F64>::Real *vb, int cap,
+                          unsigned *touched) {
   LineEval<F64, CHI> ev;
   const double UU = st.uu[q];
   const int cls = q < st.c0 ? 0 : (q < st.c1 ? 1 : 2);
-  auto put = [&](int slot, double X) { vb[(size_t)slot * cap + q] = ev(X, st.lv, st.sqrt14); };
+  // value of slot `slot` at offset X; `site` is marked as touched when the
+  // unit keeps a touched-site map (sites of grid k: edge e -> e, mid m ->
+  // ntk + m; finest point i -> i - 2)
+  auto put = [&](int slot, int site, double X) {
+    vb[(size_t)slot * cap + q] = ev(X, st.lv, st.sqrt14);
+    if (touched) atomicOr(touched + (site >> 5), 1u << (site & 31));
+  };
   if (k <= 9) {
     const double hk = h_k(k), hk1 = h_k(k - 1), hn = h_k(k + 1);
     const int ntk = nt_k(k);
@@ -680,36 +686,36 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
       ev.init(st, q);
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        if (te[d]) put(d, bL + (double)d * hk);
+        if (te[d]) put(d, n - 1 - d, bL + (double)d * hk);
 #pragma unroll
       for (int d = 0; d < 2; ++d)
-        if (tm[d]) put(3 + d, (bL + (double)d * hk) + hn);
+        if (tm[d]) put(3 + d, ntk + n - 1 - d, (bL + (double)d * hk) + hn);
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        if (re[d]) put(5 + d, bV + (double)d * hk);
+        if (re[d]) put(5 + d, ntk - nv + 1 + d, bV + (double)d * hk);
 #pragma unroll
       for (int d = 0; d < 2; ++d)
-        if (rm[d]) put(8 + d, (bV + (double)d * hk) + hn);
+        if (rm[d]) put(8 + d, ntk + ntk + 2 - nv + d, (bV + (double)d * hk) + hn);
     } else if (cls == 0) {
       if (UU > -hk1) { // D = -UU < H_{k-1}: cells 1 and 2 (leftLBL labels 20-28, 121-129)
         ev.init(st, q);
         const bool own = -UU >= hk;
-        if (own) put(0, UU);      // e = 0: P(1)
-        put(1, UU - hk);          // e = 1: L(1) when own, P(2)
-        put(2, UU - hk1);         // e = 2: L(2)
-        if (own) put(3, UU - hn); // M(1)
-        put(4, (UU - hk) - hn);   // M(2)
+        if (own) put(0, 0, UU);            // e = 0: P(1)
+        put(1, 1, UU - hk);                // e = 1: L(1) when own, P(2)
+        put(2, 2, UU - hk1);               // e = 2: L(2)
+        if (own) put(3, ntk + 1, UU - hn); // M(1)
+        put(4, ntk + 2, (UU - hk) - hn);   // M(2)
       }
     } else {
       const double U = UU - DELTA_WV;
       if (U < hk1) { // cells ntk and ntk-1 (rightLBL labels 60-69, 131-139)
         ev.init(st, q);
         const bool own = U >= hk;
-        if (own) put(0, U);       // e = ntk: L(ntk)
-        put(1, U + hk);           // e = ntk-1: L(ntk-1), P(ntk) when own
-        put(2, U + hk1);          // e = ntk-2: P(ntk-1)
-        if (own) put(3, U + hn);  // M(ntk)
-        put(4, (U + hk) + hn);    // M(ntk-1)
+        if (own) put(0, ntk, U);               // e = ntk: L(ntk)
+        put(1, ntk - 1, U + hk);               // e = ntk-1: L(ntk-1), P(ntk) when own
+        put(2, ntk - 2, U + hk1);              // e = ntk-2: P(ntk-1)
+        if (own) put(3, ntk + ntk, U + hn);    // M(ntk)
+        put(4, ntk + ntk - 1, (U + hk) + hn);  // M(ntk-1)
       }
     }
   } else {
@@ -721,32 +727,36 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
 #pragma unroll
       for (int d = 0; d < 7; ++d) { // left fine loop (LineGridCalc.f90:332-339): i = ni+1-d
         const int i = ni + 1 - d;
-        if (i >= 2 && i <= NT && ni < 4 * ((i - 2) / 4) + 8) put(d, b0 + (double)d * H);
+        if (i >= 2 && i <= NT && ni < 4 * ((i - 2) / 4) + 8) put(d, i - 2, b0 + (double)d * H);
       }
 #pragma unroll
       for (int d = 0; d < 8; ++d) { // right fine loop (LineGridCalc.f90:485-490): i = ni+2+d
         const int i = ni + 2 + d;
-        if (i >= 2 && i <= NT && nv9 < (NT - i) / 4 + 2) put(7 + d, b0 - (double)(1 + d) * H);
+        if (i >= 2 && i <= NT && nv9 < (NT - i) / 4 + 2) put(7 + d, i - 2, b0 - (double)(1 + d) * H);
       }
     } else if (cls == 0) {
       if (UU > -H9) { // leftLBL label 29: RK(2..5)
         ev.init(st, q);
-        put(0, UU - H);
-        put(1, (UU - H) - H);
-        put(2, (UU + H) - H9);
-        put(3, UU - H9);
+        put(0, 0, UU - H);
+        put(1, 1, (UU - H) - H);
+        put(2, 2, (UU + H) - H9);
+        put(3, 3, UU - H9);
       }
     } else {
       const double U = UU - DELTA_WV;
       if (U < H9) { // rightLBL label 69: RK(NT..NT-3)
         ev.init(st, q);
-        put(0, U);
-        put(1, U + H);
-        put(2, (U + H) + H);
-        put(3, (U + H9) - H);
+        put(0, NT - 2, U);
+        put(1, NT - 3, U + H);
+        put(2, NT - 4, (U + H) + H);
+        put(3, NT - 5, (U + H9) - H);
       }
     }
   }
+}
+
+__device__ __forceinline__ bool is_touched(const unsigned *touched, int site) {
+  return (touched[site >> 5] >> (site & 31)) & 1u;
 }
 
 // The site half reads the slot values of up to GB lines per batch, loads
@@ -1118,36 +1128,62 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   // there (units staged in shared memory only), else this block's global slice
   Real *vb_g = (Real *)p.vbuf + (size_t)blockIdx.x * p.vbuf_stride;
   Real *vb_s = (Real *)(fine_smem + (size_t)p.smem_cap * (24 + 3 * sizeof(Real) + 4));
+  // sparse units (few near lines) keep a map of the sites with at least one
+  // contribution in the current pass (bit per site); the site half then
+  // skips the others, which are zero
+  __shared__ unsigned s_touched[(NT + 31) / 32];
+  const bool sparse = st.m < p.sparse_lines;
+  unsigned *touched = sparse ? s_touched : nullptr;
   long long t_line = 0, t_site = 0;
   for (int k = 1; k <= 10; ++k) {
+    if (sparse) {
+      for (int w = threadIdx.x; w < (NT + 31) / 32; w += blockDim.x) s_touched[w] = 0u;
+      __syncthreads();
+    }
     const bool vsm = staged_smem && (k <= 9 ? 10 : NSLOT) <= p.vsm_rows;
     Real *vb = vsm ? vb_s : vb_g;
     const int vcap = vsm ? p.smem_cap : p.vbuf_cap;
     const long long t0 = pc ? clock64() : 0;
-    for (int q = threadIdx.x; q < st.m; q += blockDim.x) line_pass<F64, CHI>(st, q, k, vb, vcap);
+    for (int q = threadIdx.x; q < st.m; q += blockDim.x) line_pass<F64, CHI>(st, q, k, vb, vcap, touched);
     __syncthreads();
     const long long t1 = pc ? clock64() : 0;
-    if (k <= COOP_K) {
-      const int lane = threadIdx.x & 31, nsite = 2 * nt_k(k) + 1;
-      for (int site = warp_id(); site < nsite; site += blockDim.x >> 5) {
-        if (site <= nt_k(k)) gather_edge<F64>(st, k, site, vb, vcap, scr, lane, 32);
-        else gather_mid<F64>(st, k, site - nt_k(k), vb, vcap, scr, lane, 32);
-      }
-    } else if (k <= 9) {
-      const int ntk = nt_k(k), nsite = 2 * ntk + 1;
-      for (int site = threadIdx.x; site < nsite; site += blockDim.x) {
-        if (site <= ntk) gather_edge<F64>(st, k, site, vb, vcap, scr, 0, 1);
-        else gather_mid<F64>(st, k, site - ntk, vb, vcap, scr, 0, 1);
+    if (k <= 9) {
+      const int ntk = nt_k(k), nsite = 2 * ntk + 1, cb = base_k(k) - NT0;
+      const bool coop = k <= p.coop_k;
+      const int lane = coop ? (threadIdx.x & 31) : 0;
+      const int first = coop ? warp_id() : threadIdx.x, step = coop ? (blockDim.x >> 5) : blockDim.x;
+      for (int site = first; site < nsite; site += step) {
+        if (sparse && !is_touched(s_touched, site)) { // no contribution: zero accumulators
+          if (lane == 0) {
+            if (site <= ntk) {
+              if (site >= 1) scr[SCR_FINE_L + cb + site - 1] = (Real)0;
+              if (site <= ntk - 1) scr[SCR_FINE_P + cb + site] = (Real)0;
+            } else {
+              scr[SCR_FINE_M + cb + site - ntk - 1] = (Real)0;
+            }
+          }
+          continue;
+        }
+        if (coop) {
+          if (site <= ntk) gather_edge<F64>(st, k, site, vb, vcap, scr, lane, 32);
+          else gather_mid<F64>(st, k, site - ntk, vb, vcap, scr, lane, 32);
+        } else {
+          if (site <= ntk) gather_edge<F64>(st, k, site, vb, vcap, scr, 0, 1);
+          else gather_mid<F64>(st, k, site - ntk, vb, vcap, scr, 0, 1);
+        }
       }
     } else {
-      for (int i = 2 + threadIdx.x; i <= NT; i += blockDim.x) gather_point<F64>(st, i, vb, vcap, scr);
+      for (int i = 2 + threadIdx.x; i <= NT; i += blockDim.x) {
+        if (sparse && !is_touched(s_touched, i - 2)) scr[SCR_RK + i - 2] = (Real)0;
+        else gather_point<F64>(st, i, vb, vcap, scr);
+      }
     }
     __syncthreads();
     if (pc && threadIdx.x == 0) {
       const long long t2 = clock64();
       t_line += t1 - t0;
       t_site += t2 - t1;
-      if (k == COOP_K) pc[3] = t2;
+      if (k == 3) pc[3] = t2;
       if (k == 6) pc[6] = t2;
       if (k == 9) pc[7] = t2;
     }

@@ -98,6 +98,8 @@ struct FineParams {
   int vbuf_cap;                  // lines per slot row in vbuf
   int grid;                      // persistent blocks
   int vsm_rows;                  // slot-buffer rows held in shared memory (0, 10 or NSLOT)
+  int sparse_lines;              // units with fewer staged lines skip untouched sites
+  int coop_k;                    // grids 1..coop_k: one warp per site in the site half
 };
 
 struct CascadeParams {

@@ -361,6 +361,8 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   fn.order = nullptr;
   fn.grid = 1;
   fn.vsm_rows = 0;
+  fn.coop_k = 3;
+  fn.sparse_lines = 1024;
   fn.vbuf = base + OFF_VB;
   fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
   fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
