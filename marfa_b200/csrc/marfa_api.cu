@@ -35,6 +35,7 @@ struct Tune {
   int far_chunk = 4096;    // lines per far-kernel block
   int coop_k = 3;          // fine grids whose sites are summed by one warp each
   int sparse_lines = 1024; // units with fewer near lines skip untouched sites
+  int small_block_lines = 512; // batches whose units all have fewer near lines use small blocks
 };
 
 struct marfa_ctx {
@@ -579,7 +580,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.gstage_cap = max_near > fn.smem_cap ? (max_near + 255) / 256 * 256 : 0;
     fn.gstage_bytes = fn.gstage_cap ? fine_smem_bytes(fn.gstage_cap, f64) : 0;
     int resident = 0;
-    CK(fine_plan(run->precision, chi, fn.smem_cap, &fn.vsm_rows, &resident), "fine occupancy");
+    fn.block_threads = fine_block_threads(run->precision, max_near, ctx->tune.small_block_lines);
+    CK(fine_plan(run->precision, chi, fn.block_threads, fn.smem_cap, &fn.vsm_rows, &resident), "fine occupancy");
     if (fn.gstage_cap) {
       CK(ensure(ctx->b_gstage, (size_t)resident * fn.gstage_bytes), "alloc staging");
       fn.gstage = ctx->b_gstage.p;

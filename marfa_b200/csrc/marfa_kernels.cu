@@ -1149,7 +1149,7 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     const long long t1 = pc ? clock64() : 0;
     if (k <= 9) {
       const int ntk = nt_k(k), nsite = 2 * ntk + 1, cb = base_k(k) - NT0;
-      const bool coop = k <= p.coop_k;
+      const bool coop = k <= p.coop_k && !sparse; // few lines per site in sparse units
       const int lane = coop ? (threadIdx.x & 31) : 0;
       const int first = coop ? warp_id() : threadIdx.x, step = coop ? (blockDim.x >> 5) : blockDim.x;
       for (int site = first; site < nsite; site += step) {
@@ -1197,8 +1197,8 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
 
 // Persistent: every block takes units from the work queue until it is empty
 // (units in the given order, most near lines first).
-template <bool F64, int CHI>
-__global__ void __launch_bounds__(fine_threads(F64), 1) fine_kernel(FineParams p) {
+template <bool F64, int CHI, int TH>
+__global__ void __launch_bounds__(TH, TH == 256 ? 4 : 1) fine_kernel(FineParams p) {
   extern __shared__ __align__(16) unsigned char fine_smem[];
   __shared__ int s_unit;
   for (;;) {
@@ -1552,22 +1552,34 @@ cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t 
   return cudaGetLastError();
 }
 
+// Block size: fine_threads(F64) threads for dense units (the passes have
+// many sites and lines), SMALL_TH for workloads whose units have few near
+// lines: those are latency bound per unit, and small blocks put several
+// units on every SM.
+constexpr int SMALL_TH = 256;
+
+template <bool F64, int CHI, int TH>
+static cudaError_t fine_launch_th(const FineParams &p, cudaStream_t st) {
+  const size_t smem = fine_smem_bytes(p.smem_cap, F64, p.vsm_rows);
+  cudaError_t e = cudaFuncSetAttribute(fine_kernel<F64, CHI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fine_kernel<F64, CHI, TH><<<p.grid, TH, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
 template <bool F64, int CHI>
 static cudaError_t fine_launch(const FineParams &p, cudaStream_t st) {
-  const size_t smem = fine_smem_bytes(p.smem_cap, F64, p.vsm_rows);
-  cudaError_t e = cudaFuncSetAttribute(fine_kernel<F64, CHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  fine_kernel<F64, CHI><<<p.grid, fine_threads(F64), smem, st>>>(p);
-  return cudaGetLastError();
+  return p.block_threads == SMALL_TH ? fine_launch_th<F64, CHI, SMALL_TH>(p, st)
+                                     : fine_launch_th<F64, CHI, fine_threads(F64)>(p, st);
 }
 
 // Shared-memory plan of the fine kernel for `smem_cap` staged lines: the
 // most slot-buffer rows (NSLOT, 10 or 0) that fit beside the staging area,
 // and the resident blocks of the persistent grid.
-template <bool F64, int CHI>
-static cudaError_t fine_occupancy(int smem_cap, int *rows, int *blocks) {
+template <bool F64, int CHI, int TH>
+static cudaError_t fine_occupancy_th(int smem_cap, int *rows, int *blocks) {
   cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI>);
+  cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI, TH>);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0, optin = 0;
   if ((e = cudaGetDevice(&dev))) return e;
@@ -1578,13 +1590,19 @@ static cudaError_t fine_occupancy(int smem_cap, int *rows, int *blocks) {
   for (int r : {NSLOT, 10})
     if (fine_smem_bytes(smem_cap, F64, r) <= room) { *rows = r; break; }
   const size_t smem = fine_smem_bytes(smem_cap, F64, *rows);
-  if ((e = cudaFuncSetAttribute(fine_kernel<F64, CHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+  if ((e = cudaFuncSetAttribute(fine_kernel<F64, CHI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
     return e;
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fine_kernel<F64, CHI>, fine_threads(F64), smem)))
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fine_kernel<F64, CHI, TH>, TH, smem)))
     return e;
   *blocks = (per_sm < 1 ? 1 : per_sm) * sms;
   return cudaSuccess;
+}
+
+template <bool F64, int CHI>
+static cudaError_t fine_occupancy(int threads, int smem_cap, int *rows, int *blocks) {
+  return threads == SMALL_TH ? fine_occupancy_th<F64, CHI, SMALL_TH>(smem_cap, rows, blocks)
+                             : fine_occupancy_th<F64, CHI, fine_threads(F64)>(smem_cap, rows, blocks);
 }
 
 template <bool F64>
@@ -1598,12 +1616,12 @@ static cudaError_t fine_dispatch(const FineParams &p, int chi, cudaStream_t st) 
 }
 
 template <bool F64>
-static cudaError_t fine_occ_dispatch(int chi, int smem_cap, int *rows, int *blocks) {
+static cudaError_t fine_occ_dispatch(int chi, int threads, int smem_cap, int *rows, int *blocks) {
   switch (chi) {
-  case CHI_TONKOV: return fine_occupancy<F64, CHI_TONKOV>(smem_cap, rows, blocks);
-  case CHI_POLLACK: return fine_occupancy<F64, CHI_POLLACK>(smem_cap, rows, blocks);
-  case CHI_PERRIN: return fine_occupancy<F64, CHI_PERRIN>(smem_cap, rows, blocks);
-  default: return fine_occupancy<F64, CHI_NONE>(smem_cap, rows, blocks);
+  case CHI_TONKOV: return fine_occupancy<F64, CHI_TONKOV>(threads, smem_cap, rows, blocks);
+  case CHI_POLLACK: return fine_occupancy<F64, CHI_POLLACK>(threads, smem_cap, rows, blocks);
+  case CHI_PERRIN: return fine_occupancy<F64, CHI_PERRIN>(threads, smem_cap, rows, blocks);
+  default: return fine_occupancy<F64, CHI_NONE>(threads, smem_cap, rows, blocks);
   }
 }
 
@@ -1613,9 +1631,13 @@ size_t fine_smem_bytes(int cap, bool f64, int vsm_rows) {
 }
 size_t fine_vbuf_elems(int cap) { return (size_t)NSLOT * cap; }
 
-cudaError_t fine_plan(int precision, int chi, int smem_cap, int *vsm_rows, int *blocks) {
-  return precision == 0 ? fine_occ_dispatch<true>(chi, smem_cap, vsm_rows, blocks)
-                        : fine_occ_dispatch<false>(chi, smem_cap, vsm_rows, blocks);
+int fine_block_threads(int precision, int max_near, int small_below) {
+  return max_near < small_below ? SMALL_TH : fine_threads(precision == 0);
+}
+
+cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, int *vsm_rows, int *blocks) {
+  return precision == 0 ? fine_occ_dispatch<true>(chi, threads, smem_cap, vsm_rows, blocks)
+                        : fine_occ_dispatch<false>(chi, threads, smem_cap, vsm_rows, blocks);
 }
 
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st) {

@@ -100,6 +100,7 @@ struct FineParams {
   int vsm_rows;                  // slot-buffer rows held in shared memory (0, 10 or NSLOT)
   int sparse_lines;              // units with fewer staged lines skip untouched sites
   int coop_k;                    // grids 1..coop_k: one warp per site in the site half
+  int block_threads;             // threads per block (fine_block_threads)
 };
 
 struct CascadeParams {
@@ -199,8 +200,11 @@ cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st)
 // `vsm_rows` slot-buffer rows of `cap` values
 size_t fine_smem_bytes(int cap, bool f64, int vsm_rows = 0);
 size_t fine_vbuf_elems(int cap);
+// block size of the fine kernel for a batch whose units have at most
+// `max_near` near lines (small blocks below `small_below` lines)
+int fine_block_threads(int precision, int max_near, int small_below);
 // slot-buffer rows that fit in shared memory and the persistent grid size
-cudaError_t fine_plan(int precision, int chi, int smem_cap, int *vsm_rows, int *blocks);
+cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, int *vsm_rows, int *blocks);
 cudaError_t fma_peak(bool f64, double *flops_per_s);
 cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st);
 cudaError_t launch_count(const CountParams &p, cudaStream_t st);

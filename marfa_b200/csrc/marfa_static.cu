@@ -363,6 +363,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   fn.vsm_rows = 0;
   fn.coop_k = 3;
   fn.sparse_lines = 1024;
+  fn.block_threads = fine_block_threads(run->precision, 1 << 30, 0);
   fn.vbuf = base + OFF_VB;
   fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
   fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
