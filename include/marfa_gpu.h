@@ -145,6 +145,40 @@ int marfa_compute_device(marfa_ctx *ctx, const marfa_run *run, int n_profiles,
                          float *device_out, void *stream);
 int marfa_synchronize(marfa_ctx *ctx);
 
+/* A compute call captured once into a CUDA graph and replayed for new
+ * profiles of the same shape.  The reference recomputes from scratch for
+ * every profile (main.f90:81-180); this is the batched form for many
+ * profiles.  marfa_graph_create computes the records of the given profiles
+ * into `device_out` (like marfa_compute_device, then waits), then captures the
+ * same launches -- prep, sort, far, persistent fine kernel with its device
+ * work queue, cascade -- into a graph.  marfa_graph_launch takes new
+ * pressure / temperature / density arrays of the same level counts, stages
+ * them and launches the graph on `stream` (NULL = the context's stream)
+ * without waiting; the records go to the same `device_out`.  It returns
+ * MARFA_E_ARG when the launch plan no longer matches the capture (the
+ * context's buffers were grown by a larger computation in between, or the
+ * near-line counts of the new profile need larger staging): create a new
+ * graph then.  One graph per context at a time is launched on its stream. */
+typedef struct marfa_graph marfa_graph;
+int marfa_graph_create(marfa_ctx *ctx, const marfa_run *run, int n_profiles,
+                       const int *level_counts, const double *pressure,
+                       const double *temperature, const double *density, float *device_out,
+                       marfa_graph **out);
+int marfa_graph_launch(marfa_graph *graph, const double *pressure, const double *temperature,
+                       const double *density, void *stream);
+void marfa_graph_destroy(marfa_graph *graph);
+
+/* Chooses the context's launch parameters that do not change the method --
+ * lines per far-kernel block (far_chunk: 2048, 4096 or 8192) and the number of
+ * coarse fine grids whose accumulators are summed by a whole warp (coop_k:
+ * 1..5) -- by timing every candidate on up to four levels of the given
+ * profile, keeps the fastest in the context and returns it.  Results change
+ * only by summation order (far-line sums are split differently).  No
+ * reference counterpart (the reference has no launch parameters). */
+int marfa_autotune(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *pressure,
+                   const double *temperature, const double *density, int *far_chunk,
+                   int *coop_k);
+
 /* Replaces the reference intensities S and air-broadening coefficients
  * gamma_air of every line by double values (either pointer may be NULL: back
  * to the database record's float value).  The reference reads both from the

@@ -22,7 +22,8 @@ EXPORTS = (
     "marfa_record_number", "marfa_compute", "marfa_compute_batched", "marfa_compute_device",
     "marfa_synchronize", "marfa_eval_count", "marfa_debug_accumulators", "marfa_last_timings",
     "marfa_plan_windows", "marfa_measure_fma_peak", "marfa_compute_record_static",
-    "marfa_ctx_set_line_params", "marfa_vjp",
+    "marfa_ctx_set_line_params", "marfa_vjp", "marfa_graph_create", "marfa_graph_launch",
+    "marfa_graph_destroy", "marfa_autotune",
 )
 
 
@@ -77,6 +78,10 @@ def load():
                                             P, ctypes.c_char_p, ctypes.c_size_t]),
         "marfa_ctx_set_line_params": (I, [P, P, P]),
         "marfa_vjp": (I, [P, ctypes.POINTER(MarfaRun), P, P, P, I, P, P, P, P, P]),
+        "marfa_graph_create": (I, [P, ctypes.POINTER(MarfaRun), I, P, P, P, P, P, ctypes.POINTER(P)]),
+        "marfa_graph_launch": (I, [P, P, P, P, P]),
+        "marfa_graph_destroy": (None, [P]),
+        "marfa_autotune": (I, [P, ctypes.POINTER(MarfaRun), I, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

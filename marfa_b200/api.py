@@ -146,6 +146,30 @@ class Context:
     def synchronize(self):
         self._check(self._lib.marfa_synchronize(self._h))
 
+    def graph(self, run: Run, level_counts, pressure, temperature, density, device_ptr: int) -> "Graph":
+        """Compute into the device buffer at `device_ptr` and capture the
+        launches into a CUDA graph, replayed by Graph.launch for new profiles
+        of the same level counts."""
+        P, T, n = _f64(pressure), _f64(temperature), _f64(density)
+        counts = np.ascontiguousarray(level_counts, dtype=np.int32)
+        r = run.c()
+        h = ctypes.c_void_p()
+        self._check(self._lib.marfa_graph_create(
+            self._h, ctypes.byref(r), len(counts), counts.ctypes.data, P.ctypes.data, T.ctypes.data,
+            n.ctypes.data, ctypes.c_void_p(device_ptr), ctypes.byref(h)))
+        return Graph(self, h)
+
+    def autotune(self, run: Run, pressure, temperature, density) -> dict:
+        """Time the launch-parameter candidates on a few levels of this
+        profile and keep the fastest for later calls."""
+        P, T, n = _f64(pressure), _f64(temperature), _f64(density)
+        fc, ck = ctypes.c_int(), ctypes.c_int()
+        r = run.c()
+        self._check(self._lib.marfa_autotune(self._h, ctypes.byref(r), len(P), P.ctypes.data,
+                                             T.ctypes.data, n.ctypes.data, ctypes.byref(fc),
+                                             ctypes.byref(ck)))
+        return {"far_chunk": fc.value, "coop_k": ck.value}
+
     @property
     def n_lines(self) -> int:
         return len(self._lines)
@@ -208,6 +232,30 @@ class Context:
         self._check(self._lib.marfa_last_timings(self._h, t.ctypes.data))
         return dict(zip(("prep", "sort", "far", "fine", "cascade", "total", "launches",
                          "far_launches"), t.tolist()))
+
+
+class Graph:
+    """A captured compute call (marfa_graph_*)."""
+
+    def __init__(self, ctx: Context, handle):
+        self._ctx = ctx
+        self._h = handle
+
+    def launch(self, pressure, temperature, density, stream: int = 0):
+        P, T, n = _f64(pressure), _f64(temperature), _f64(density)
+        self._ctx._check(self._ctx._lib.marfa_graph_launch(self._h, P.ctypes.data, T.ctypes.data,
+                                                           n.ctypes.data, ctypes.c_void_p(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._ctx._lib.marfa_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _ptr(a) -> int:

@@ -41,6 +41,7 @@ struct Tune {
 struct marfa_ctx {
   int device = 0;
   Tune tune;
+  unsigned long long alloc_gen = 0; // counts (re)allocations of the work buffers
   cudaStream_t stream = nullptr;
   int64_t n_lines = 0;
   std::vector<double> nu;  // host copy of the sorted centres (window scan)
@@ -57,7 +58,7 @@ struct marfa_ctx {
   int *d_err = nullptr;
   // grow-only work buffers
   DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
-      b_out, b_out64, b_dump, b_count, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order;
+      b_out, b_out64, b_dump, b_count, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order, b_tune;
   std::string err;
   // pinned staging of the per-call host tables (see Staging)
   void *pinned = nullptr;
@@ -106,6 +107,13 @@ cudaError_t ensure(DevBuf &b, size_t bytes) {
   cudaError_t e = cudaMalloc(&b.p, want);
   if (e == cudaSuccess) b.cap = want;
   return e;
+}
+
+// Grow-only buffer of the context; a reallocation invalidates captured graphs.
+cudaError_t ensure(marfa_ctx *ctx, DevBuf &b, size_t bytes) {
+  if (bytes <= b.cap) return cudaSuccess;
+  ++ctx->alloc_gen;
+  return ensure(b, bytes);
 }
 
 void release(DevBuf &b) {
@@ -306,7 +314,24 @@ struct VjpOut {
   double *dS = nullptr, *dgair = nullptr, *dT = nullptr, *dP = nullptr;
 };
 
+// Fine-kernel launch plan of one chunk of levels.
+struct FineChunk {
+  int max_near = 0, smem_cap = 0, gstage_cap = 0, block_threads = 0, vsm_rows = 0, resident = 0;
+  size_t gstage_bytes = 0;
+};
+
+// Capture of one compute call into a CUDA graph, and its replays.
+struct GraphCtl {
+  bool replay = false;             // false: capture during this call
+  int Lc = 0, UB = 0;              // chunking of the captured call
+  std::vector<long long> sig;      // launch plan of the captured call
+  unsigned long long alloc_gen = 0;
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;
+};
+
 struct Outputs {
+  GraphCtl *graph = nullptr;     // capture into / replay of a CUDA graph
   const VjpOut *vjp = nullptr;   // adjoint instead of records
   float *host_out = nullptr;     // host records (copied per level chunk)
   double *host_out64 = nullptr;
@@ -359,29 +384,33 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   const size_t unit_bytes = (size_t)SCR_STRIDE * elem * (adj ? 2 : 1); // + gradient scratch
   const size_t scr_budget = std::max<size_t>(unit_bytes, std::min<size_t>((size_t)4 << 30, (free_b + ctx->b_scr.cap) / 5));
   int UB = (int)std::max<size_t>(1, std::min<size_t>((size_t)Lc * nsub, scr_budget / unit_bytes));
-
-  CK(ensure(ctx->b_nus, (size_t)Lc * N * 8), "alloc nus");
-  CK(ensure(ctx->b_gen, (size_t)Lc * N * sizeof(LineGen)), "alloc gen");
-  CK(ensure(ctx->b_hot, (size_t)Lc * N * (f64 ? sizeof(Hot64) : sizeof(Hot32))), "alloc hot");
-  CK(ensure(ctx->b_rank, (size_t)Lc * N * 8), "alloc rank");
-  CK(ensure(ctx->b_snu, (size_t)Lc * N * 8), "alloc snu");
-  CK(ensure(ctx->b_sidx, (size_t)Lc * N * 4), "alloc sidx");
-  CK(ensure(ctx->b_far, (size_t)Lc * std::max(C, 1) * NFAR * 8), "alloc far");
-  CK(ensure(ctx->b_scr, (size_t)UB * SCR_STRIDE * elem), "alloc scratch");
-  if (adj) {
-    CK(ensure(ctx->b_gscr, (size_t)UB * SCR_STRIDE * 8), "alloc gradient scratch");
-    CK(ensure(ctx->b_aux, (size_t)Lc * N * sizeof(LineAux)), "alloc line partials");
+  if (o.graph && o.graph->replay) { // the captured chunking
+    Lc = o.graph->Lc;
+    UB = o.graph->UB;
   }
-  CK(ensure(ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
-  CK(ensure(ctx->b_margin, (size_t)n_levels * 8), "alloc margin");
-  if (!o.dev_out && !adj) CK(ensure(ctx->b_out, (size_t)Lc * nsub * NT * 4), "alloc out");
-  if (o.host_out64) CK(ensure(ctx->b_out64, (size_t)Lc * nsub * NT * 8), "alloc out64");
-  if (o.host_dump) CK(ensure(ctx->b_dump, (size_t)(NT + 3 * NCELLS) * 8), "alloc dump");
+
+  CK(ensure(ctx, ctx->b_nus, (size_t)Lc * N * 8), "alloc nus");
+  CK(ensure(ctx, ctx->b_gen, (size_t)Lc * N * sizeof(LineGen)), "alloc gen");
+  CK(ensure(ctx, ctx->b_hot, (size_t)Lc * N * (f64 ? sizeof(Hot64) : sizeof(Hot32))), "alloc hot");
+  CK(ensure(ctx, ctx->b_rank, (size_t)Lc * N * 8), "alloc rank");
+  CK(ensure(ctx, ctx->b_snu, (size_t)Lc * N * 8), "alloc snu");
+  CK(ensure(ctx, ctx->b_sidx, (size_t)Lc * N * 4), "alloc sidx");
+  CK(ensure(ctx, ctx->b_far, (size_t)Lc * std::max(C, 1) * NFAR * 8), "alloc far");
+  CK(ensure(ctx, ctx->b_scr, (size_t)UB * SCR_STRIDE * elem), "alloc scratch");
+  if (adj) {
+    CK(ensure(ctx, ctx->b_gscr, (size_t)UB * SCR_STRIDE * 8), "alloc gradient scratch");
+    CK(ensure(ctx, ctx->b_aux, (size_t)Lc * N * sizeof(LineAux)), "alloc line partials");
+  }
+  CK(ensure(ctx, ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
+  CK(ensure(ctx, ctx->b_margin, (size_t)n_levels * 8), "alloc margin");
+  if (!o.dev_out && !adj) CK(ensure(ctx, ctx->b_out, (size_t)Lc * nsub * NT * 4), "alloc out");
+  if (o.host_out64) CK(ensure(ctx, ctx->b_out64, (size_t)Lc * nsub * NT * 8), "alloc out64");
+  if (o.host_dump) CK(ensure(ctx, ctx->b_dump, (size_t)(NT + 3 * NCELLS) * 8), "alloc dump");
   // window and chunk tables
   const size_t win_bytes = (size_t)nsub * (8 + 8 + 8 + 8) + (size_t)(nsub + 1) * 4;
-  CK(ensure(ctx->b_win, win_bytes), "alloc windows");
+  CK(ensure(ctx, ctx->b_win, win_bytes), "alloc windows");
   const size_t chunk_bytes = (size_t)std::max(C, 1) * (4 + 8 + 8);
-  CK(ensure(ctx->b_chunks, chunk_bytes), "alloc chunks");
+  CK(ensure(ctx, ctx->b_chunks, chunk_bytes), "alloc chunks");
 
   char *wb = (char *)ctx->b_win.p;
   double *d_s = (double *)wb;
@@ -425,7 +454,39 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       std::stable_sort(o_, o_ + nu_, [&](int x, int y) { return nbound[base + u0 + x] > nbound[base + u0 + y]; });
     }
   }
-  CK(ensure(ctx->b_order, order_all.size() * 4), "alloc order");
+  CK(ensure(ctx, ctx->b_order, order_all.size() * 4), "alloc order");
+
+  // launch plan of the fine kernel per chunk of levels: staged lines per
+  // block in shared memory (units with more near lines stage in a global
+  // slice of their block), block size, slot rows in shared memory, grid
+  std::vector<FineChunk> fchunks;
+  size_t gstage_need = 0, vbuf_need = 0;
+  for (int l0 = 0; l0 < n_levels; l0 += Lc) {
+    const int units = std::min(Lc, n_levels - l0) * nsub;
+    FineChunk fc;
+    fc.max_near = *std::max_element(nbound.begin() + (size_t)l0 * nsub, nbound.begin() + (size_t)l0 * nsub + units);
+    if (fc.max_near > 65535) // line indices of one unit are 16-bit in the fine kernel's bin table
+      return set_err(ctx, MARFA_E_CAPACITY, "%d lines within 1 cm-1 of one subinterval (at most 65535)",
+                     fc.max_near);
+    const int smem_max = f64 ? 4096 : 2688;
+    fc.smem_cap = std::max(256, std::min(smem_max, (fc.max_near + 127) / 128 * 128));
+    fc.gstage_cap = fc.max_near > fc.smem_cap ? (fc.max_near + 255) / 256 * 256 : 0;
+    fc.gstage_bytes = fc.gstage_cap ? fine_smem_bytes(fc.gstage_cap, f64) : 0;
+    fc.block_threads = fine_block_threads(run->precision, fc.max_near, ctx->tune.small_block_lines);
+    CK(fine_plan(run->precision, chi, fc.block_threads, fc.smem_cap, &fc.vsm_rows, &fc.resident), "fine occupancy");
+    gstage_need = std::max(gstage_need, (size_t)fc.resident * fc.gstage_bytes);
+    vbuf_need = std::max(vbuf_need, (size_t)fc.resident *
+                                        fine_vbuf_elems(std::max(fc.smem_cap, fc.gstage_cap)) * elem);
+    fchunks.push_back(fc);
+  }
+  if (gstage_need) CK(ensure(ctx, ctx->b_gstage, gstage_need), "alloc staging");
+  CK(ensure(ctx, ctx->b_vbuf, vbuf_need), "alloc slot buffers");
+  CK(ensure(ctx, ctx->b_queue, 256), "alloc queue");
+
+  // a captured graph replays only the launch plan it was captured with
+  std::vector<long long> sig = {Lc, UB, (long long)ctx->alloc_gen};
+  for (const FineChunk &fc : fchunks)
+    sig.insert(sig.end(), {fc.smem_cap, fc.gstage_cap, fc.block_threads, fc.vsm_rows, fc.resident});
 
   Staging sg{ctx, st};
   const size_t stage_bytes = 4 * Staging::room((size_t)nsub * 8) + Staging::room((size_t)(nsub + 1) * 4) +
@@ -445,6 +506,22 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   CK(sg.put(d_margin, margin.data(), n_levels * 8), "h2d margin");
   CK(sg.put(ctx->b_order.p, order_all.data(), order_all.size() * 4), "h2d order");
   CK(sg.end(), "staging event");
+  if (o.graph && o.graph->replay) {
+    if (sig != o.graph->sig)
+      return set_err(ctx, MARFA_E_ARG, "the graph was captured for another launch plan (line buffers grown or "
+                                       "near-line counts changed): create a new graph");
+    CK(cudaGraphLaunch(o.graph->exec, st), "graph launch");
+    ctx->marks.clear();
+    ctx->launches = o.graph->launches;
+    ctx->far_launches = 0;
+    return MARFA_OK;
+  }
+  if (o.graph) {
+    o.graph->sig = sig;
+    o.graph->Lc = Lc;
+    o.graph->UB = UB;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "begin capture");
+  }
   CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st), "memset err");
 
   WindowTable win{d_s, d_e, d_lo, d_hi, nsub};
@@ -458,6 +535,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   auto mark = [&](int fam, cudaEvent_t a, cudaEvent_t b) { ctx->marks.push_back({fam, {a, b}}); };
   size_t ev_used = 0;
   auto next_event = [&]() -> cudaEvent_t {
+    if (o.graph) return nullptr; // no timing events inside a graph
     if (ev_used == ctx->events.size()) {
       cudaEvent_t e;
       if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
@@ -563,34 +641,23 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     // diagnostics: MARFA_PHASE_CLOCK=<file> records clock64 marks of every
     // fine-kernel block of the first batch (int64 [units][10]: start, staged, grid 0, grids 1-3, end, near count, grids 4-6, grids 7-9, line-half and site-half cycles) into <file>
     const char *clock_path = std::getenv("MARFA_PHASE_CLOCK");
-    if (clock_path && l0 == 0) {
-      CK(ensure(ctx->b_count, (size_t)units * 10 * 8), "alloc clock");
+    if (clock_path && l0 == 0 && !o.graph) {
+      CK(ensure(ctx, ctx->b_count, (size_t)units * 10 * 8), "alloc clock");
       CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * 10 * 8, st), "memset clock");
       fn.phase_clock = (long long *)ctx->b_count.p;
     }
-    const int max_near = units ? *std::max_element(nbound.begin() + (size_t)l0 * nsub,
-                                                   nbound.begin() + (size_t)l0 * nsub + units) : 0;
-    if (max_near > 65535) // line indices of one unit are 16-bit in the fine kernel's bin table
-      return set_err(ctx, MARFA_E_CAPACITY, "%d lines within 1 cm-1 of one subinterval (at most 65535)", max_near);
-    // staged lines per block in shared memory; units with more near lines
-    // stage in a global slice of their block
-    const int smem_max = f64 ? 4096 : 2688;
-    fn.smem_cap = std::max(256, std::min(smem_max, (max_near + 127) / 128 * 128));
-    fn.gstage = nullptr;
-    fn.gstage_cap = max_near > fn.smem_cap ? (max_near + 255) / 256 * 256 : 0;
-    fn.gstage_bytes = fn.gstage_cap ? fine_smem_bytes(fn.gstage_cap, f64) : 0;
-    int resident = 0;
-    fn.block_threads = fine_block_threads(run->precision, max_near, ctx->tune.small_block_lines);
-    CK(fine_plan(run->precision, chi, fn.block_threads, fn.smem_cap, &fn.vsm_rows, &resident), "fine occupancy");
-    if (fn.gstage_cap) {
-      CK(ensure(ctx->b_gstage, (size_t)resident * fn.gstage_bytes), "alloc staging");
-      fn.gstage = ctx->b_gstage.p;
-    }
+    const FineChunk &fc = fchunks[l0 / Lc];
+    const int max_near = fc.max_near;
+    fn.smem_cap = fc.smem_cap;
+    fn.gstage_cap = fc.gstage_cap;
+    fn.gstage_bytes = fc.gstage_bytes;
+    fn.gstage = fc.gstage_cap ? ctx->b_gstage.p : nullptr;
+    fn.block_threads = fc.block_threads;
+    fn.vsm_rows = fc.vsm_rows;
+    const int resident = fc.resident;
     fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
     fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
-    CK(ensure(ctx->b_vbuf, (size_t)resident * fn.vbuf_stride * elem), "alloc slot buffers");
     fn.vbuf = ctx->b_vbuf.p;
-    CK(ensure(ctx->b_queue, 256), "alloc queue");
     fn.queue = (int *)ctx->b_queue.p;
     fn.coop_k = ctx->tune.coop_k;
     fn.sparse_lines = ctx->tune.sparse_lines;
@@ -701,6 +768,15 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   if (o.host_dump)
     CK(cudaMemcpyAsync(o.host_dump, ctx->b_dump.p, (size_t)(NT + 3 * NCELLS) * 8, cudaMemcpyDeviceToHost, st),
        "d2h dump");
+  if (o.graph) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamEndCapture(st, &g), "end capture");
+    const cudaError_t e = cudaGraphInstantiate(&o.graph->exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e, "graph instantiate");
+    o.graph->launches = ctx->launches;
+    return MARFA_OK;
+  }
   if (o.dev_out) return MARFA_OK; // asynchronous path: caller synchronises
   CK(cudaStreamSynchronize(st), "stream sync");
   int herr = 0;
@@ -845,7 +921,7 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
   DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
                   &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
                   &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_gstage, &ctx->b_aux,
-                  &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order};
+                  &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order, &ctx->b_tune};
   for (DevBuf *b : bs) release(*b);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
@@ -949,8 +1025,8 @@ int marfa_vjp(marfa_ctx *ctx, const marfa_run *run, const double *pressure, cons
   cudaStream_t st = ctx->stream;
   try {
     const size_t ncot = (size_t)n_levels * nsub * NT;
-    CK(ensure(ctx->b_cot, std::max<size_t>(ncot, 1) * 8), "alloc cotangent");
-    CK(ensure(ctx->b_grad, ((size_t)2 * N + 2 * n_levels) * 8), "alloc gradients");
+    CK(ensure(ctx, ctx->b_cot, std::max<size_t>(ncot, 1) * 8), "alloc cotangent");
+    CK(ensure(ctx, ctx->b_grad, ((size_t)2 * N + 2 * n_levels) * 8), "alloc gradients");
     double *g = (double *)ctx->b_grad.p;
     VjpOut v;
     v.cot = (const double *)ctx->b_cot.p;
@@ -973,6 +1049,132 @@ int marfa_vjp(marfa_ctx *ctx, const marfa_run *run, const double *pressure, cons
   } catch (...) {
     return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
   }
+}
+
+struct marfa_graph {
+  marfa_ctx *ctx = nullptr;
+  marfa_run run{};
+  int total = 0;
+  float *dev_out = nullptr;
+  GraphCtl ctl;
+};
+
+int marfa_graph_create(marfa_ctx *ctx, const marfa_run *run, int n_profiles, const int *level_counts,
+                       const double *pressure, const double *temperature, const double *density,
+                       float *device_out, marfa_graph **out) {
+  if (!ctx || !out) return MARFA_E_ARG;
+  *out = nullptr;
+  if (!run || !device_out) return set_err(ctx, MARFA_E_ARG, "null argument");
+  int total = 0, rc = total_levels(ctx, n_profiles, level_counts, total);
+  if (rc) return rc;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+  marfa_graph *g = new (std::nothrow) marfa_graph();
+  if (!g) return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
+  g->ctx = ctx;
+  g->run = *run;
+  g->total = total;
+  g->dev_out = device_out;
+  try {
+    // one eager call allocates every buffer (no allocation may happen while
+    // the stream is captured) and computes the records; the second call is
+    // captured
+    Outputs o;
+    o.dev_out = device_out;
+    rc = run_levels(ctx, run, total, pressure, temperature, density, o, ctx->stream);
+    if (!rc) rc = marfa_synchronize(ctx);
+    if (!rc) {
+      o.graph = &g->ctl;
+      rc = run_levels(ctx, run, total, pressure, temperature, density, o, ctx->stream);
+    }
+  } catch (...) {
+    rc = set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+    cudaGraph_t dead = nullptr; // a failed capture: close it and drop the graph
+    cudaStreamEndCapture(ctx->stream, &dead);
+    if (dead) cudaGraphDestroy(dead);
+  }
+  if (rc || !g->ctl.exec) {
+    marfa_graph_destroy(g);
+    return rc ? rc : set_err(ctx, MARFA_E_CUDA, "graph capture produced no graph");
+  }
+  g->ctl.replay = true;
+  *out = g;
+  return MARFA_OK;
+}
+
+int marfa_graph_launch(marfa_graph *g, const double *pressure, const double *temperature,
+                       const double *density, void *stream) {
+  if (!g) return MARFA_E_ARG;
+  if (cudaSetDevice(g->ctx->device) != cudaSuccess) return set_err(g->ctx, MARFA_E_CUDA, "cudaSetDevice");
+  Outputs o;
+  o.dev_out = g->dev_out;
+  o.graph = &g->ctl;
+  try {
+    return run_levels(g->ctx, &g->run, g->total, pressure, temperature, density, o,
+                      stream ? (cudaStream_t)stream : g->ctx->stream);
+  } catch (...) {
+    return set_err(g->ctx, MARFA_E_NOMEM, "host allocation failed");
+  }
+}
+
+void marfa_graph_destroy(marfa_graph *g) {
+  if (!g) return;
+  if (g->ctl.exec) cudaGraphExecDestroy(g->ctl.exec);
+  delete g;
+}
+
+int marfa_autotune(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *pressure,
+                   const double *temperature, const double *density, int *far_chunk, int *coop_k) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!run || n_levels < 1 || !pressure || !temperature || !density)
+    return set_err(ctx, MARFA_E_ARG, "null argument");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
+  // sample: up to four levels spread over the profile, every subinterval
+  std::vector<int> pick;
+  for (int j = 0; j < std::min(4, n_levels); ++j) {
+    const int l = n_levels == 1 ? 0 : (int)std::lround((double)j * (n_levels - 1) / (std::min(4, n_levels) - 1));
+    if (pick.empty() || pick.back() != l) pick.push_back(l);
+  }
+  std::vector<double> P, T, n;
+  for (int l : pick) {
+    P.push_back(pressure[l]);
+    T.push_back(temperature[l]);
+    n.push_back(density[l]);
+  }
+  const int L = (int)pick.size();
+  const int nsub = marfa_num_subintervals(run->start_wv, run->end_wv);
+  CK(ensure(ctx, ctx->b_tune, std::max<size_t>((size_t)L * nsub * NT * 4, 4)), "alloc tuning records");
+  const Tune keep = ctx->tune;
+  Tune best = keep;
+  double best_ms = 1e300;
+  for (int fcv : {2048, 4096, 8192})
+    for (int ck : {1, 2, 3, 4, 5}) {
+      ctx->tune.far_chunk = fcv;
+      ctx->tune.coop_k = ck;
+      double ms = 1e300;
+      for (int rep = 0; rep < 3; ++rep) { // the first call also grows buffers
+        Outputs o;
+        o.dev_out = (float *)ctx->b_tune.p;
+        int rc = run_levels(ctx, run, L, P.data(), T.data(), n.data(), o, ctx->stream);
+        if (!rc) rc = marfa_synchronize(ctx);
+        if (rc) {
+          ctx->tune = keep;
+          return rc;
+        }
+        double t[8];
+        if (rep > 0 && marfa_last_timings(ctx, t) == MARFA_OK) ms = std::min(ms, t[5]);
+      }
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = ctx->tune;
+      }
+    }
+  ctx->tune = best;
+  if (far_chunk) *far_chunk = best.far_chunk;
+  if (coop_k) *coop_k = best.coop_k;
+  return MARFA_OK;
 }
 
 int marfa_synchronize(marfa_ctx *ctx) {
@@ -1006,12 +1208,12 @@ int marfa_eval_count(marfa_ctx *ctx, const marfa_run *run, int n_levels, const d
       if (far_evals) far_evals[l] = 0;
     }
     if (C == 0) return MARFA_OK;
-    CK(ensure(ctx->b_nus, (size_t)N * 8), "alloc nus");
-    CK(ensure(ctx->b_gen, (size_t)N * sizeof(LineGen)), "alloc gen");
-    CK(ensure(ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
-    CK(ensure(ctx->b_win, (size_t)nsub * 32), "alloc windows");
-    CK(ensure(ctx->b_chunks, (size_t)C * 20), "alloc chunks");
-    CK(ensure(ctx->b_count, (size_t)C * 16), "alloc count");
+    CK(ensure(ctx, ctx->b_nus, (size_t)N * 8), "alloc nus");
+    CK(ensure(ctx, ctx->b_gen, (size_t)N * sizeof(LineGen)), "alloc gen");
+    CK(ensure(ctx, ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
+    CK(ensure(ctx, ctx->b_win, (size_t)nsub * 32), "alloc windows");
+    CK(ensure(ctx, ctx->b_chunks, (size_t)C * 20), "alloc chunks");
+    CK(ensure(ctx, ctx->b_count, (size_t)C * 16), "alloc count");
     double *d_s = (double *)ctx->b_win.p, *d_e = d_s + nsub;
     int64_t *d_cb = (int64_t *)ctx->b_chunks.p, *d_ce = d_cb + C;
     int *d_cs = (int *)(d_ce + C);
