@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2],
+                    help="1: the Venus PT-table set (the headline); 2: the uneven batch of 64 "
+                         "profiles through one autotuned, graph-captured launch sequence")
+    ap.add_argument("--scale", type=float, default=1.0, help="config 2 only: fraction of its size")
     return ap.parse_args()
 
 
@@ -324,6 +328,66 @@ def run_b200(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_uneven(args, rank, local_rank):
+    """The uneven batch: 64 synthetic profiles of 10-100 levels (P log-uniform
+    1e-4..100 atm, T uniform 150-750 K) over an H2O-like list of 30,000 lines,
+    10-3000 cm-1, cutoff 25 cm-1, FP32c.  The launch parameters are autotuned
+    on the first profile, the computation of all profiles is captured once in
+    a CUDA graph, and every timed step replays it (restaging the profile
+    tables).  The records stay on the device (86 GB at full size)."""
+    import torch
+    from marfa_b200 import build as B, synth
+    from marfa_b200.api import Context, Run
+    if rank != 0:
+        return
+    B.build()
+    torch.cuda.set_device(local_rank)
+    w = synth.config(2, args.scale)
+    counts = [len(p.pressure) for p in w.profiles]
+    cat = lambda f: np.concatenate([np.asarray(getattr(p, f), dtype=np.float64) for p in w.profiles])
+    P, T, n = cat("pressure"), cat("temperature"), cat("density")
+    L = sum(counts)
+    ctx = Context(w.lines, tips_table(), device=local_rank)
+    run = Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule, chi=w.chi,
+              precision="fp32c")
+    evals = int(ctx.eval_count(run, P, T, n).sum())
+    p0 = w.profiles[0]
+    tune = ctx.autotune(run, p0.pressure, p0.temperature, p0.density)
+    out = torch.empty((L, run.n_sub, 20481), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    g = ctx.graph(run, counts, P, T, n, out.data_ptr())
+    for _ in range(args.warmup):
+        g.launch(P, T, n, stream.cuda_stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        g.launch(P, T, n, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ctx.synchronize()
+    tm = ctx.timings()
+    print(json.dumps({
+        "metric": "line-grid evals/s (uneven batch, FP32c, graph replay)", "value": evals / (ms * 1e-3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 (compensated) + fp64 offsets", "data": "synthetic",
+        "config": {"workload": "uneven-64-profiles-h2o-30k-lines-10-3000cm-1-cutoff25",
+                   "scale": args.scale, "profiles": len(counts), "levels": L,
+                   "subintervals": run.n_sub, "lines": int(len(w.lines) - 1),
+                   "record_bytes_on_device": int(out.numel() * 4)},
+        "evals_per_step": evals, "autotuned": tune, "graph_launches_per_step": 1,
+        "gpu_launches_per_step": int(tm["launches"]), "clocks": clk,
+    }))
+    g.close()
+    ctx.close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -331,6 +395,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+    elif args.config == 2:
+        run_uneven(args, rank, local_rank)
     else:
         run_b200(args, rank, world, local_rank)
 
