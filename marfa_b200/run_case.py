@@ -23,6 +23,8 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--shape", default="voigt", choices=["voigt", "one", "absx"])
     ap.add_argument("--iters", type=int, default=2)
+    ap.add_argument("--vjp", action="store_true",
+                    help="run the adjoint (FP64) for a Gaussian cotangent instead of the forward")
     args = ap.parse_args(argv)
 
     import torch
@@ -38,6 +40,13 @@ def main(argv=None):
     ctx = Context(w.lines, read_tips(data_path("TIPS_subset.dat")))
     run = Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule, chi=w.chi,
               precision=args.precision, shape=args.shape)
+    if args.vjp:
+        cot = np.random.default_rng(3).standard_normal((len(P), run.n_sub, 20481))
+        for it in range(args.iters):
+            g = ctx.vjp(run, P, T, n, cot)
+            print(json.dumps({"iter": it, "dT": g["dT"].tolist(), "dP": g["dP"].tolist()}), flush=True)
+        ctx.close()
+        return
     out = torch.empty((len(P), run.n_sub, 20481), dtype=torch.float32, device="cuda")
     for it in range(args.iters):
         ctx.compute_device(run, [len(P)], P, T, n, out.data_ptr(), 0)
