@@ -637,8 +637,8 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
   const double UU = st.uu[q];
   const int cls = q < st.c0 ? 0 : (q < st.c1 ? 1 : 2);
   // value of slot `slot` at offset X; `site` is marked as touched when the
-  // unit keeps a touched-site map (sites of grid k: edge e -> e, mid m ->
-  // ntk + m; finest point i -> i - 2)
+  // unit keeps a touched-site map (sites of grid k: cell e -> e for its edge
+  // e and its mid e; finest point i -> i - 2)
   auto put = [&](int slot, int site, double X) {
     vb[(size_t)slot * cap + q] = ev(X, st.lv, st.sqrt14);
     if (touched) atomicOr(touched + (site >> 5), 1u << (site & 31));
@@ -689,13 +689,13 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
         if (te[d]) put(d, n - 1 - d, bL + (double)d * hk);
 #pragma unroll
       for (int d = 0; d < 2; ++d)
-        if (tm[d]) put(3 + d, ntk + n - 1 - d, (bL + (double)d * hk) + hn);
+        if (tm[d]) put(3 + d, n - 1 - d, (bL + (double)d * hk) + hn);
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         if (re[d]) put(5 + d, ntk - nv + 1 + d, bV + (double)d * hk);
 #pragma unroll
       for (int d = 0; d < 2; ++d)
-        if (rm[d]) put(8 + d, ntk + ntk + 2 - nv + d, (bV + (double)d * hk) + hn);
+        if (rm[d]) put(8 + d, ntk + 2 - nv + d, (bV + (double)d * hk) + hn);
     } else if (cls == 0) {
       if (UU > -hk1) { // D = -UU < H_{k-1}: cells 1 and 2 (leftLBL labels 20-28, 121-129)
         ev.init(st, q);
@@ -703,8 +703,8 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
         if (own) put(0, 0, UU);            // e = 0: P(1)
         put(1, 1, UU - hk);                // e = 1: L(1) when own, P(2)
         put(2, 2, UU - hk1);               // e = 2: L(2)
-        if (own) put(3, ntk + 1, UU - hn); // M(1)
-        put(4, ntk + 2, (UU - hk) - hn);   // M(2)
+        if (own) put(3, 1, UU - hn);       // M(1)
+        put(4, 2, (UU - hk) - hn);         // M(2)
       }
     } else {
       const double U = UU - DELTA_WV;
@@ -714,8 +714,8 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
         if (own) put(0, ntk, U);               // e = ntk: L(ntk)
         put(1, ntk - 1, U + hk);               // e = ntk-1: L(ntk-1), P(ntk) when own
         put(2, ntk - 2, U + hk1);              // e = ntk-2: P(ntk-1)
-        if (own) put(3, ntk + ntk, U + hn);    // M(ntk)
-        put(4, ntk + ntk - 1, (U + hk) + hn);  // M(ntk-1)
+        if (own) put(3, ntk, U + hn);          // M(ntk)
+        put(4, ntk - 1, (U + hk) + hn);        // M(ntk-1)
       }
     }
   } else {
@@ -763,25 +763,32 @@ __device__ __forceinline__ bool is_touched(const unsigned *touched, int site) {
 // first, sums after, so that the loads of a batch are in flight together.
 constexpr int GB = 2;
 
-// Site half: edge e (0..ntk) of grid k -> L(e), P(e+1).  Lanes of a warp
-// stride over the lines when stride > 1 (lane 0 stores the warp sum).
+// Site half: cell e (0..ntk) of grid k -> L(e), P(e+1) of edge e and M(e) of
+// mid e.  The mid takes exactly the lines that give L(e) (its walk conditions
+// are those of L(e), at offset X + H_{k+1}), so one pass over the edge's line
+// runs serves all three accumulators.  Lanes of a warp stride over the lines
+// when stride > 1 (lane 0 stores the warp sums).
 template <bool F64>
-__device__ void gather_edge(const NearStore<F64> &st, int k, int e, const typename NearStore<F64>::Real *vb,
+__device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typename NearStore<F64>::Real *vb,
                             int cap, void *scr, int lane, int stride) {
   using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
   const int ntk = nt_k(k), sh = 11 - k;
-  const bool hasL = e >= 1, hasP = e <= ntk - 1;
+  const bool hasL = e >= 1, hasP = e <= ntk - 1; // hasL is also "has M"
   const int wl = 2 * ((e + 1) / 2) + 2, wp = 2 * ((e + 2) / 2) + 2; // walk ends of e, e+1 in bins
-  Acc<F64> aL, aP;
+  Acc<F64> aL, aP, aM;
   aL.init();
   aP.init();
-  Real f[GB];
+  aM.init();
+  Real f[GB], g[GB];
   bool tl[GB], tp[GB];
   auto flush = [&]() {
 #pragma unroll
     for (int j = 0; j < GB; ++j) {
-      if (tl[j]) aL.add(f[j]);
+      if (tl[j]) {
+        aL.add(f[j]);
+        aM.add(g[j]);
+      }
       if (tp[j]) aP.add(f[j]);
     }
   };
@@ -795,6 +802,7 @@ __device__ void gather_edge(const NearStore<F64> &st, int k, int e, const typena
         tl[j] = hasL && n >= e + 1 && n < wl;
         tp[j] = hasP && n >= e + 2 && n < wp;
         f[j] = (tl[j] || tp[j]) ? vb[(size_t)(n - 1 - e) * cap + q] : (Real)0;
+        g[j] = tl[j] ? vb[(size_t)(3 + n - 1 - e) * cap + q] : (Real)0;
       }
       flush();
     }
@@ -811,6 +819,7 @@ __device__ void gather_edge(const NearStore<F64> &st, int k, int e, const typena
         tl[j] = hasL && nv >= rL + 1 && nv < wrl;
         tp[j] = hasP && nv >= rP + 1 && nv < wrp;
         f[j] = (tl[j] || tp[j]) ? vb[(size_t)(5 + e - (ntk - nv + 1)) * cap + q] : (Real)0;
+        g[j] = tl[j] ? vb[(size_t)(8 + e - (ntk + 2 - nv)) * cap + q] : (Real)0;
       }
       flush();
     }
@@ -826,6 +835,7 @@ __device__ void gather_edge(const NearStore<F64> &st, int k, int e, const typena
         tl[j] = in && ((e == 1 && own) || e == 2);
         tp[j] = in && ((e == 0 && own) || e == 1);
         f[j] = (tl[j] || tp[j]) ? vb[(size_t)e * cap + q] : (Real)0;
+        g[j] = tl[j] ? vb[(size_t)(2 + e) * cap + q] : (Real)0;
       }
       flush();
     }
@@ -841,90 +851,23 @@ __device__ void gather_edge(const NearStore<F64> &st, int k, int e, const typena
         tl[j] = in && ((e == ntk && own) || e == ntk - 1);
         tp[j] = in && ((e == ntk - 1 && own) || e == ntk - 2);
         f[j] = (tl[j] || tp[j]) ? vb[(size_t)(ntk - e) * cap + q] : (Real)0;
+        g[j] = tl[j] ? vb[(size_t)(3 + ntk - e) * cap + q] : (Real)0;
       }
       flush();
     }
   }
   const bool coop = stride > 1;
   const double vL = coop_sum(aL.value(), coop), vP = coop_sum(aP.value(), coop);
+  const double vM = coop_sum(aM.value(), coop);
   if (lane == 0) {
     Real *o = (Real *)scr;
     const int cb = base_k(k) - NT0;
-    if (hasL) o[SCR_FINE_L + cb + e - 1] = (Real)vL;
+    if (hasL) {
+      o[SCR_FINE_L + cb + e - 1] = (Real)vL;
+      o[SCR_FINE_M + cb + e - 1] = (Real)vM;
+    }
     if (hasP) o[SCR_FINE_P + cb + e] = (Real)vP;
   }
-}
-
-// Site half: mid m (1..ntk) of grid k -> M(m).
-template <bool F64>
-__device__ void gather_mid(const NearStore<F64> &st, int k, int m, const typename NearStore<F64>::Real *vb,
-                           int cap, void *scr, int lane, int stride) {
-  using Real = typename NearStore<F64>::Real;
-  const double hk = h_k(k), hk1 = h_k(k - 1);
-  const int ntk = nt_k(k), sh = 11 - k;
-  Acc<F64> aM;
-  aM.init();
-  Real f[GB];
-  bool on[GB];
-  auto flush = [&]() {
-#pragma unroll
-    for (int j = 0; j < GB; ++j)
-      if (on[j]) aM.add(f[j]);
-  };
-  { // left walk: bins m+1, m+2
-    const int wm = 2 * ((m + 1) / 2) + 2;
-    const int q0 = st.lbL(k, m + 1), q1 = st.lbL(k, m + 3);
-    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        const int n = q < q1 ? st.n11[q] >> sh : -1;
-        on[j] = n >= m + 1 && n < wm;
-        f[j] = on[j] ? vb[(size_t)(3 + n - 1 - m) * cap + q] : (Real)0;
-      }
-      flush();
-    }
-  }
-  { // right walk: V bins r+1, r+2 with r = ntk+1-m
-    const int r = ntk + 1 - m, wr = 2 * ((r + 1) / 2) + 2;
-    const int q0 = st.lbV(k, r + 3), q1 = st.lbV(k, r + 1);
-    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        const int nv = q < q1 ? st.nv11[q] >> sh : -1;
-        on[j] = nv >= r + 1 && nv < wr;
-        f[j] = on[j] ? vb[(size_t)(8 + m - (ntk + 2 - nv)) * cap + q] : (Real)0;
-      }
-      flush();
-    }
-  }
-  if (m <= 2) {
-    const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
-    for (int qb = q0 + lane; qb < st.c0; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        on[j] = q < st.c0 && (m == 2 || -st.uu[q] >= hk);
-        f[j] = on[j] ? vb[(size_t)(2 + m) * cap + q] : (Real)0;
-      }
-      flush();
-    }
-  }
-  if (m >= ntk - 1) {
-    const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
-    for (int qb = st.c1 + lane; qb < q1; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        on[j] = q < q1 && (m == ntk - 1 || (st.uu[q] - DELTA_WV) >= hk);
-        f[j] = on[j] ? vb[(size_t)(3 + ntk - m) * cap + q] : (Real)0;
-      }
-      flush();
-    }
-  }
-  const double vM = coop_sum(aM.value(), stride > 1);
-  if (lane == 0) ((Real *)scr)[SCR_FINE_M + base_k(k) - NT0 + m - 1] = (Real)vM;
 }
 
 // Site half: finest point i (2..NT) -> RK(i).
@@ -1148,29 +1091,23 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     __syncthreads();
     const long long t1 = pc ? clock64() : 0;
     if (k <= 9) {
-      const int ntk = nt_k(k), nsite = 2 * ntk + 1, cb = base_k(k) - NT0;
+      const int ntk = nt_k(k), nsite = ntk + 1, cb = base_k(k) - NT0;
       const bool coop = k <= p.coop_k && !sparse; // few lines per site in sparse units
       const int lane = coop ? (threadIdx.x & 31) : 0;
       const int first = coop ? warp_id() : threadIdx.x, step = coop ? (blockDim.x >> 5) : blockDim.x;
-      for (int site = first; site < nsite; site += step) {
-        if (sparse && !is_touched(s_touched, site)) { // no contribution: zero accumulators
+      for (int e = first; e < nsite; e += step) {
+        if (sparse && !is_touched(s_touched, e)) { // no contribution: zero accumulators
           if (lane == 0) {
-            if (site <= ntk) {
-              if (site >= 1) scr[SCR_FINE_L + cb + site - 1] = (Real)0;
-              if (site <= ntk - 1) scr[SCR_FINE_P + cb + site] = (Real)0;
-            } else {
-              scr[SCR_FINE_M + cb + site - ntk - 1] = (Real)0;
+            if (e >= 1) {
+              scr[SCR_FINE_L + cb + e - 1] = (Real)0;
+              scr[SCR_FINE_M + cb + e - 1] = (Real)0;
             }
+            if (e <= ntk - 1) scr[SCR_FINE_P + cb + e] = (Real)0;
           }
           continue;
         }
-        if (coop) {
-          if (site <= ntk) gather_edge<F64>(st, k, site, vb, vcap, scr, lane, 32);
-          else gather_mid<F64>(st, k, site - ntk, vb, vcap, scr, lane, 32);
-        } else {
-          if (site <= ntk) gather_edge<F64>(st, k, site, vb, vcap, scr, 0, 1);
-          else gather_mid<F64>(st, k, site - ntk, vb, vcap, scr, 0, 1);
-        }
+        if (coop) gather_cell<F64>(st, k, e, vb, vcap, scr, lane, 32);
+        else gather_cell<F64>(st, k, e, vb, vcap, scr, 0, 1);
       }
     } else {
       for (int i = 2 + threadIdx.x; i <= NT; i += blockDim.x) {
