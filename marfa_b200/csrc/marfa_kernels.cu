@@ -213,7 +213,7 @@ struct ChiPieces {
 };
 
 template <bool F64, int CHI>
-__global__ void __launch_bounds__(256, F64 ? 2 : 3) far_kernel(FarParams p) {
+__global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
   const int item = blockIdx.x;
   const int l = item / p.n_chunks;
   const int ci = item - l * p.n_chunks;
