@@ -43,6 +43,10 @@ struct marfa_ctx {
   Tune tune;
   unsigned long long alloc_gen = 0; // counts (re)allocations of the work buffers
   cudaStream_t stream = nullptr;
+  // records to host memory: copies of one chunk of levels overlap the
+  // computation of the next (two device halves, copy stream, events)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t rec_ready[2] = {nullptr, nullptr}, rec_copied[2] = {nullptr, nullptr};
   int64_t n_lines = 0;
   std::vector<double> nu;  // host copy of the sorted centres (window scan)
   double smax = 0.0;       // largest reference intensity
@@ -200,34 +204,33 @@ int plan_windows(const double *nu, int64_t n, double start_wv, double end_wv, do
                  std::vector<int64_t> &hi, int &bad) {
   const int nsub = marfa_num_subintervals(start_wv, end_wv);
   bad = -1;
-  // determineStartingSpectralLine (main.f90:196-248)
+  // determineStartingSpectralLine (main.f90:196-248): the first record with
+  // nu > start - cutoff.  The line list is sorted, so the reference's linear
+  // scans are binary searches here, with the same results.
   int64_t start_idx = 0;
   double start_line = nu[0];
   if (start_wv > cut) {
     const double ext = start_wv - cut;
-    int64_t i = 0;
-    while (nu[i] <= ext)
-      if (++i >= n) return MARFA_E_DB;
-    start_idx = i;
-    start_line = nu[i];
+    start_idx = std::upper_bound(nu, nu + n, ext) - nu;
+    if (start_idx >= n) return MARFA_E_DB;
+    start_line = nu[start_idx];
   }
-  // SUBINTERVALS_LOOP with the lblScheme window recurrence
+  // SUBINTERVALS_LOOP with the lblScheme window recurrence: the scan from
+  // line_idx stops at the first nu >= start + 10 + cutoff; the next window
+  // starts at the last scanned line with nu <= capWV (or stays)
   int64_t line_idx = start_idx;
   double s = start_wv;
   for (int isub = 0; isub < nsub; ++isub) {
     const double ext_end = s + DELTA_WV + cut;
     double cap = (s - cut) + DELTA_WV;
     if (cap <= start_line) cap = start_line;
-    int64_t I = line_idx, next = line_idx;
-    for (;; ++I) {
-      if (I >= n) {
-        bad = isub;
-        return MARFA_E_DB;
-      }
-      const double v = nu[I];
-      if (v >= ext_end) break;
-      if (v <= cap) next = I;
+    const int64_t I = std::lower_bound(nu + line_idx, nu + n, ext_end) - nu;
+    if (I >= n) {
+      bad = isub;
+      return MARFA_E_DB;
     }
+    const int64_t last = (std::upper_bound(nu + line_idx, nu + I, cap) - nu) - 1;
+    const int64_t next = last >= line_idx ? last : line_idx;
     ss.push_back(s);
     se.push_back(s + DELTA_WV);
     lo.push_back(line_idx);
@@ -374,7 +377,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   const bool adj = o.vjp != nullptr;
   const size_t per_level = (size_t)N * (8 + sizeof(LineGen) + (f64 ? sizeof(Hot64) : sizeof(Hot32)) + 8 + 8 + 4 +
                                         (adj ? sizeof(LineAux) : 0)) +
-                           (size_t)C * NFAR * 8 + (size_t)nsub * NT * (o.dev_out || adj ? 0 : 4) +
+                           (size_t)C * NFAR * 8 + (size_t)nsub * NT * (o.dev_out || adj ? 0 : 8) +
                            (o.host_out64 ? (size_t)nsub * NT * 8 : 0);
   const size_t reuse = ctx->b_nus.cap + ctx->b_gen.cap + ctx->b_hot.cap + ctx->b_rank.cap + ctx->b_snu.cap +
                        ctx->b_sidx.cap + ctx->b_far.cap + ctx->b_out.cap + ctx->b_out64.cap;
@@ -387,6 +390,18 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   if (o.graph && o.graph->replay) { // the captured chunking
     Lc = o.graph->Lc;
     UB = o.graph->UB;
+  }
+  // host records: at least four chunks of levels, so that the copy of each
+  // overlaps the computation of the next
+  const bool host_records = o.host_out != nullptr && !adj;
+  if (host_records) {
+    Lc = std::min(Lc, std::max(1, (n_levels + 3) / 4));
+    UB = std::min(UB, Lc * nsub);
+    if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
+    for (int h = 0; h < 2; ++h) {
+      if (!ctx->rec_ready[h]) CK(cudaEventCreateWithFlags(&ctx->rec_ready[h], cudaEventDisableTiming), "event");
+      if (!ctx->rec_copied[h]) CK(cudaEventCreateWithFlags(&ctx->rec_copied[h], cudaEventDisableTiming), "event");
+    }
   }
 
   CK(ensure(ctx, ctx->b_nus, (size_t)Lc * N * 8), "alloc nus");
@@ -403,7 +418,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   }
   CK(ensure(ctx, ctx->b_lv, (size_t)n_levels * sizeof(LevelConst)), "alloc levels");
   CK(ensure(ctx, ctx->b_margin, (size_t)n_levels * 8), "alloc margin");
-  if (!o.dev_out && !adj) CK(ensure(ctx, ctx->b_out, (size_t)Lc * nsub * NT * 4), "alloc out");
+  if (!o.dev_out && !adj) CK(ensure(ctx, ctx->b_out, (size_t)2 * Lc * nsub * NT * 4), "alloc out");
   if (o.host_out64) CK(ensure(ctx, ctx->b_out64, (size_t)Lc * nsub * NT * 8), "alloc out64");
   if (o.host_dump) CK(ensure(ctx, ctx->b_dump, (size_t)(NT + 3 * NCELLS) * 8), "alloc dump");
   // window and chunk tables
@@ -620,7 +635,10 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     mark(1, e1, e2);
     mark(2, e2, e3);
 
-    float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p;
+    const int half = (l0 / Lc) & 1;
+    float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p + (size_t)half * Lc * nsub * NT;
+    // the half written now was copied out two chunks ago
+    if (host_records && l0 >= 2 * Lc) CK(cudaStreamWaitEvent(st, ctx->rec_copied[half], 0), "wait copy");
     const int out_level0 = o.dev_out ? l0 : 0;
     const int units = nl * nsub;
     // near-line counts of this chunk's units size the fine kernel's staging
@@ -755,9 +773,13 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       mark(3, f0, f1);
       mark(4, f1, f2);
     }
-    if (o.host_out)
-      CK(cudaMemcpyAsync(o.host_out + (size_t)l0 * nsub * NT, ctx->b_out.p, (size_t)nl * nsub * NT * 4,
-                         cudaMemcpyDeviceToHost, st), "d2h records");
+    if (host_records) {
+      CK(cudaEventRecord(ctx->rec_ready[half], st), "event");
+      CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->rec_ready[half], 0), "wait records");
+      CK(cudaMemcpyAsync(o.host_out + (size_t)l0 * nsub * NT, out_base, (size_t)nl * nsub * NT * 4,
+                         cudaMemcpyDeviceToHost, ctx->copy_stream), "d2h records");
+      CK(cudaEventRecord(ctx->rec_copied[half], ctx->copy_stream), "event");
+    }
     if (o.host_out64)
       CK(cudaMemcpyAsync(o.host_out64 + (size_t)l0 * nsub * NT, ctx->b_out64.p, (size_t)nl * nsub * NT * 8,
                          cudaMemcpyDeviceToHost, st), "d2h records64");
@@ -779,6 +801,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   }
   if (o.dev_out) return MARFA_OK; // asynchronous path: caller synchronises
   CK(cudaStreamSynchronize(st), "stream sync");
+  if (host_records) CK(cudaStreamSynchronize(ctx->copy_stream), "copy stream sync");
   int herr = 0;
   CK(cudaMemcpy(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost), "d2h err");
   if (herr) return set_err(ctx, herr, "device reported status %d (isotopologue or temperature outside tables)", herr);
@@ -923,6 +946,14 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
                   &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_gstage, &ctx->b_aux,
                   &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order, &ctx->b_tune};
   for (DevBuf *b : bs) release(*b);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
+  for (int h = 0; h < 2; ++h) {
+    if (ctx->rec_ready[h]) cudaEventDestroy(ctx->rec_ready[h]);
+    if (ctx->rec_copied[h]) cudaEventDestroy(ctx->rec_copied[h]);
+  }
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
