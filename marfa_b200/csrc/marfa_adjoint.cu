@@ -295,17 +295,14 @@ __global__ void __launch_bounds__(256) cascade_adjoint_kernel(CascadeAdjParams p
   double *gs = p.gscratch + (size_t)ub * SCR_STRIDE;
   __shared__ double val[1023 * 3]; // forward cell values of the subtree, grid k at sub_off(k)
   __shared__ double gv[1023 * 3];  // their gradients
-  if (threadIdx.x == 0) {
-    const double *far = p.far + ((size_t)l * p.n_chunks) * NFAR;
-    double fP = 0.0, fM = 0.0, fL = 0.0;
-    for (int c = p.sub_chunk0[sub]; c < p.sub_chunk0[sub + 1]; ++c) {
-      fP += far[(size_t)c * NFAR + 2 * (J - 1)];
-      fM += far[(size_t)c * NFAR + 2 * J - 1];
-      fL += far[(size_t)c * NFAR + 2 * J];
+  if (threadIdx.x < 32) { // grid-0 cell J as cascade_kernel forms it
+    double f[4];
+    far_cell_sums(p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
+    if (threadIdx.x == 0) {
+      val[0] = f[0] + scr[1 + J - 1];
+      val[1] = f[1] + scr[11 + J - 1];
+      val[2] = f[2] + scr[21 + J - 1];
     }
-    val[0] = fP + scr[1 + J - 1];
-    val[1] = fM + scr[11 + J - 1];
-    val[2] = fL + scr[21 + J - 1];
   }
   __syncthreads();
   // forward cascade, as cascade_kernel (same operations, same decisions)

@@ -367,4 +367,22 @@ __device__ __forceinline__ bool near_keep(double v, int64_t li, double s, double
   return UU < DELTA_WV;
 }
 
+// Far-line sums of grid-0 cell J of one unit over its far-kernel chunks
+// [c0, c1): P(J), M(J), L(J) and the RK(1) position, for the 32 lanes of one
+// warp (lanes over chunks, then a fixed-order xor reduction: every lane gets
+// the same sums, in the same order for every call).
+__device__ __forceinline__ void far_cell_sums(const double *far, int c0, int c1, int J, double (&f)[4]) {
+  f[0] = f[1] = f[2] = f[3] = 0.0;
+  for (int c = c0 + (int)(threadIdx.x & 31); c < c1; c += 32) {
+    f[0] += far[(size_t)c * NFAR + 2 * (J - 1)];
+    f[1] += far[(size_t)c * NFAR + 2 * J - 1];
+    f[2] += far[(size_t)c * NFAR + 2 * J];
+    f[3] += far[(size_t)c * NFAR];
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) f[i] += __shfl_xor_sync(0xffffffffu, f[i], off);
+}
+
 } // namespace marfa

@@ -870,55 +870,51 @@ __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typena
   }
 }
 
-// Site half: finest point i (2..NT) -> RK(i).
+// Site half of the finest pass for the four points i = 4j-2 .. 4j+1 of
+// grid-9 cell j.  They share both outer bounds: the left fine loop ends at
+// (4 floor((i-2)/4) + 8) H = (4j + 4) H and the right fine loop's V bound is
+// (floor((NT-i)/4) + 2) H9 = (5122 - j) H9, so every line of the run
+// [first V < (5122 - j) H9, first UU >= (4j + 4) H) reaches all four points:
+// point i through its left loop when floor(UU/H) >= i - 1, else through its
+// right loop.  Per point, the left-loop lines are summed first, then the
+// right-loop lines, then the near lines (the order of the point form).
 template <bool F64>
-__device__ void gather_point(const NearStore<F64> &st, int i, const typename NearStore<F64>::Real *vb, int cap,
-                             void *scr) {
+__device__ void gather_quad(const NearStore<F64> &st, int j, const typename NearStore<F64>::Real *vb, int cap,
+                            void *scr) {
   using Real = typename NearStore<F64>::Real;
   const double H9 = h_k(9);
-  Acc<F64> a;
-  a.init();
-  Real f[GB];
-  bool on[GB];
-  auto flush = [&]() {
+  const int i0 = 4 * j - 2;
+  Acc<F64> a[4];
 #pragma unroll
-    for (int j = 0; j < GB; ++j)
-      if (on[j]) a.add(f[j]);
-  };
-  const int qa = st.lbL(11, i - 1);
-  { // left fine loop: UU in [(i-1) H, (4 floor((i-2)/4) + 8) H)
-    const int qe = st.lbL(11, 4 * ((i - 2) / 4) + 8);
-    for (int qb = qa; qb < qe; qb += GB) {
+  for (int p = 0; p < 4; ++p) a[p].init();
+  const int q0 = st.lbV(9, 5122 - j), q1 = st.lbL(11, 4 * j + 4);
+  for (int q = q0; q < q1; ++q) { // left fine loops
+    const int ni = st.n11[q];
 #pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j;
-        on[j] = q < qe;
-        f[j] = on[j] ? vb[(size_t)(st.n11[q] + 1 - i) * cap + q] : (Real)0;
-      }
-      flush();
-    }
+    for (int p = 0; p < 4; ++p)
+      if (ni >= i0 + p - 1) a[p].add(vb[(size_t)(ni + 1 - i0 - p) * cap + q]);
   }
-  { // right fine loop: UU < (i-1) H and V < (floor((NT-i)/4) + 2) H9
-    const int qb0 = st.lbV(9, (NT - i) / 4 + 2);
-    for (int qb = qb0; qb < qa; qb += GB) {
+  for (int q = q0; q < q1; ++q) { // right fine loops
+    const int ni = st.n11[q];
 #pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j;
-        on[j] = q < qa;
-        f[j] = on[j] ? vb[(size_t)(7 + i - st.n11[q] - 2) * cap + q] : (Real)0;
-      }
-      flush();
-    }
+    for (int p = 0; p < 4; ++p)
+      if (ni < i0 + p - 1) a[p].add(vb[(size_t)(7 + i0 + p - ni - 2) * cap + q]);
   }
-  if (i <= 5) {
-    const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -H9; });
-    for (int q = q0; q < st.c0; ++q) a.add(vb[(size_t)(i - 2) * cap + q]);
+  if (j == 1) { // RK(2..5): near-left lines with D < H9
+    const int qn = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -H9; });
+    for (int q = qn; q < st.c0; ++q)
+#pragma unroll
+      for (int p = 0; p < 4; ++p) a[p].add(vb[(size_t)p * cap + q]);
   }
-  if (i >= NT - 3) {
-    const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= H9; });
-    for (int q = st.c1; q < q1; ++q) a.add(vb[(size_t)(NT - i) * cap + q]);
+  if (j == NBIN9) { // RK(NT-3..NT): near-right lines with U < H9
+    const int qn = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= H9; });
+    for (int q = st.c1; q < qn; ++q)
+#pragma unroll
+      for (int p = 0; p < 4; ++p) a[p].add(vb[(size_t)(NT - i0 - p) * cap + q]);
   }
-  ((Real *)scr)[SCR_RK + i - 2] = (Real)a.value();
+  Real *o = (Real *)scr;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) o[SCR_RK + i0 + p - 2] = (Real)a[p].value();
 }
 
 __device__ __forceinline__ int block_excl_scan(int v, int &total) {
@@ -1110,9 +1106,13 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
         else gather_cell<F64>(st, k, e, vb, vcap, scr, 0, 1);
       }
     } else {
-      for (int i = 2 + threadIdx.x; i <= NT; i += blockDim.x) {
-        if (sparse && !is_touched(s_touched, i - 2)) scr[SCR_RK + i - 2] = (Real)0;
-        else gather_point<F64>(st, i, vb, vcap, scr);
+      for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) {
+        if (sparse && ((s_touched[(4 * j - 4) >> 5] >> ((4 * j - 4) & 31)) & 15u) == 0u) {
+#pragma unroll
+          for (int p = 0; p < 4; ++p) scr[SCR_RK + 4 * j - 4 + p] = (Real)0;
+        } else {
+          gather_quad<F64>(st, j, vb, vcap, scr);
+        }
       }
     }
     __syncthreads();
@@ -1199,20 +1199,15 @@ __global__ void __launch_bounds__(256) cascade_kernel(CascadeParams p) {
   __shared__ double bufB[512 * 3];
   __shared__ float outb[2048];
   __shared__ double rk1;
-  if (threadIdx.x == 0) {
-    // grid-0 cell J: far-line sums over this subinterval's chunks + near part
-    const double *far = p.far + ((size_t)l * p.n_chunks) * NFAR;
-    double fP = 0.0, fM = 0.0, fL = 0.0, f0 = 0.0;
-    for (int c = p.sub_chunk0[sub]; c < p.sub_chunk0[sub + 1]; ++c) {
-      fP += far[(size_t)c * NFAR + 2 * (J - 1)];
-      fM += far[(size_t)c * NFAR + 2 * J - 1];
-      fL += far[(size_t)c * NFAR + 2 * J];
-      f0 += far[(size_t)c * NFAR];
+  if (threadIdx.x < 32) { // grid-0 cell J: far-line sums + near part
+    double f[4];
+    far_cell_sums(p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
+    if (threadIdx.x == 0) {
+      bufA[0] = (f[0] + (double)scr[1 + J - 1]) * inv;
+      bufA[1] = (f[1] + (double)scr[11 + J - 1]) * inv;
+      bufA[2] = (f[2] + (double)scr[21 + J - 1]) * inv;
+      rk1 = (f[3] + (double)scr[0]) * inv;
     }
-    bufA[0] = (fP + (double)scr[1 + J - 1]) * inv;
-    bufA[1] = (fM + (double)scr[11 + J - 1]) * inv;
-    bufA[2] = (fL + (double)scr[21 + J - 1]) * inv;
-    rk1 = (f0 + (double)scr[0]) * inv;
   }
   __syncthreads();
   double *prev = bufA, *cur = bufB;
