@@ -265,9 +265,11 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
 #pragma unroll
     for (int k = 0; k < NFAR; ++k) res[k] = acc[k];
   } else {
-    Kahan acc[NFAR];
+    // plain float sums: one thread adds FAR_CHUNK / 256 lines per position
+    // (16 at the default chunk), the block reduction then runs in double
+    float acc[NFAR];
 #pragma unroll
-    for (int k = 0; k < NFAR; ++k) acc[k].init();
+    for (int k = 0; k < NFAR; ++k) acc[k] = 0.f;
     const ChiPieces<CHI> pc(lv);
     for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
       double D;
@@ -289,10 +291,10 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
           }
           if (left) {
 #pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[k].add(F[k]);
+            for (int k = 0; k < NFAR; ++k) acc[k] += F[k];
           } else {
 #pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k].add(F[k]);
+            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k] += F[k];
           }
         } else {
           int kb[3];
@@ -324,10 +326,10 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
           }
           if (left) {
 #pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[k].add(F[k]);
+            for (int k = 0; k < NFAR; ++k) acc[k] += F[k];
           } else {
 #pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k].add(F[k]);
+            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k] += F[k];
           }
         }
       } else {
@@ -342,15 +344,15 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
         }
         if (left) {
 #pragma unroll
-          for (int k = 0; k < NFAR; ++k) acc[k].add(F[k]);
+          for (int k = 0; k < NFAR; ++k) acc[k] += F[k];
         } else {
 #pragma unroll
-          for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k].add(F[k]);
+          for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k] += F[k];
         }
       }
     }
 #pragma unroll
-    for (int k = 0; k < NFAR; ++k) res[k] = acc[k].value();
+    for (int k = 0; k < NFAR; ++k) res[k] = (double)acc[k];
   }
   block_reduce_store<NFAR>(res, p.out + ((size_t)l * p.n_chunks + ci) * NFAR);
 }
