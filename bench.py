@@ -237,13 +237,11 @@ def run_b200(args, rank, world, local_rank):
     # FP64 drop-in
     ms64, tm64, _ = timed_steps(ctx, run64, p, out64, stream, max(2, args.steps // 2), 1)
     barrier()
-    ms_max = ms32
-    if dist is not None:
-        t = torch.tensor([ms32, ms64], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max, ms64 = float(t[0]), float(t[1])
-    value = world * evals / (ms_max * 1e-3)
-    value64 = world * evals / (ms64 * 1e-3)
+    from marfa_b200.multi import reduce_step
+    ms_max, total_evals = reduce_step(ms32, evals, dist)  # slowest rank, work of all ranks
+    ms64, _ = reduce_step(ms64, evals, dist)
+    value = total_evals / (ms_max * 1e-3)
+    value64 = total_evals / (ms64 * 1e-3)
 
     # accuracy of the FP32c records against the FP64 drop-in (same workload)
     a = out32.double()
@@ -263,10 +261,8 @@ def run_b200(args, rank, world, local_rank):
     for _ in range(e2e_steps):
         ctx.compute(run32, p.pressure, p.temperature, p.density, out=host_out)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t[0])
+    e2e_ms, _ = reduce_step(e2e_s * 1e3, evals, dist)
+    e2e_s = e2e_ms * 1e-3
     h2d = 3 * L * 8
     d2h = host_out.numel() * 4
 
@@ -317,7 +313,7 @@ def run_b200(args, rank, world, local_rank):
             "far_kernel_tflops": far_roof,
             "fma_peak_tflops": {"fp32": fp32_peak[0] / 1e12, "fp64": fp64_peak[0] / 1e12},
             "cpu_baseline": cpu,
-            "e2e": {"value": world * evals / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e": {"value": total_evals / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clk,
