@@ -47,6 +47,10 @@ struct marfa_ctx {
   // computation of the next (two device halves, copy stream, events)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t rec_ready[2] = {nullptr, nullptr}, rec_copied[2] = {nullptr, nullptr};
+  // per level of the last call with host records: kernel time and copy time
+  // (ms), which shape the level chunks of the next such call
+  double rec_compute_ms = 0.0, rec_copy_ms = 0.0;
+  int sm_count = 0;
   int64_t n_lines = 0;
   std::vector<double> nu;  // host copy of the sorted centres (window scan)
   double smax = 0.0;       // largest reference intensity
@@ -343,6 +347,47 @@ struct Outputs {
   int dump_level = -1, dump_sub = -1;
 };
 
+// Level chunks of one call, as sizes in order.  Without host records:
+// chunks of Lc levels.  With records copied to host memory the copy of each
+// chunk overlaps the computation of the next, and r = copy time / kernel
+// time per level (measured on the previous such call) shapes the chunks:
+// r < 1 (kernels dominate): sizes shrink by r towards the end, from m0
+// levels at the end, so that the copy left after the last kernel is short
+// and every copy fits under the next chunk's kernels; r >= 1 (the copy
+// dominates): a first chunk of m0 levels starts the copy engine early.
+// Without a measurement: four equal chunks.  No chunk exceeds Lc.
+static std::vector<int> level_chunk_sizes(int n, int Lc, bool host_records, double r, int m0) {
+  std::vector<int> sz;
+  if (n <= 0) return sz;
+  auto uniform = [&](int from, int q) {
+    for (int l = from; l < n; l += q) sz.push_back(std::min(q, n - l));
+  };
+  if (!host_records) {
+    uniform(0, Lc);
+    return sz;
+  }
+  const int q4 = std::min(Lc, std::max(1, (n + 3) / 4));
+  m0 = std::max(1, std::min(m0, q4));
+  if (!(r > 0.0) || n < 4) {
+    uniform(0, q4);
+  } else if (r < 1.0) {
+    std::vector<int> back; // last chunk first
+    double want = m0;
+    int sum = 0;
+    while (sum < n) {
+      const int c = std::min({Lc, n - sum, std::max(1, (int)std::ceil(want - 1e-9))});
+      back.push_back(c);
+      sum += c;
+      want = want / std::max(r, 0.25);
+    }
+    sz.assign(back.rbegin(), back.rend());
+  } else {
+    sz.push_back(m0);
+    uniform(m0, std::min(Lc, std::max(m0, (n - m0 + 3) / 4)));
+  }
+  return sz;
+}
+
 // The whole computation for a flat list of levels.
 int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *P,
                const double *T, const double *dens, const Outputs &o, cudaStream_t st) {
@@ -394,8 +439,17 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   // host records: at least four chunks of levels, so that the copy of each
   // overlaps the computation of the next
   const bool host_records = o.host_out != nullptr && !adj;
+  if (host_records && !ctx->sm_count)
+    CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device), "device attribute");
+  // chunk boundaries: chunk c holds levels [lb[c], lb[c + 1])
+  const int m0 = (2 * std::max(ctx->sm_count, 1) + nsub - 1) / nsub; // two blocks per SM at least
+  const double r_copy = ctx->rec_compute_ms > 0.0 ? ctx->rec_copy_ms / ctx->rec_compute_ms : 0.0;
+  const std::vector<int> csz = level_chunk_sizes(n_levels, Lc, host_records, r_copy, m0);
+  std::vector<int> lb(1, 0);
+  for (int c : csz) lb.push_back(lb.back() + c);
+  const int n_chunks = (int)csz.size();
   if (host_records) {
-    Lc = std::min(Lc, std::max(1, (n_levels + 3) / 4));
+    Lc = *std::max_element(csz.begin(), csz.end()); // largest chunk: sizes the record halves
     UB = std::min(UB, Lc * nsub);
     if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
     for (int h = 0; h < 2; ++h) {
@@ -460,8 +514,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       const auto b0 = std::upper_bound(a0, ctx->nu.end(), hi);
       nbound[(size_t)l * nsub + isub] = (int)(b0 - a0);
     }
-  for (int l0 = 0; l0 < n_levels; l0 += Lc) {
-    const int base = l0 * nsub, units = std::min(Lc, n_levels - l0) * nsub;
+  for (int c = 0; c < n_chunks; ++c) {
+    const int base = lb[c] * nsub, units = (lb[c + 1] - lb[c]) * nsub;
     for (int u0 = 0; u0 < units; u0 += UB) {
       const int nu_ = std::min(UB, units - u0);
       int *o_ = order_all.data() + base + u0;
@@ -476,8 +530,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   // slice of their block), block size, slot rows in shared memory, grid
   std::vector<FineChunk> fchunks;
   size_t gstage_need = 0, vbuf_need = 0;
-  for (int l0 = 0; l0 < n_levels; l0 += Lc) {
-    const int units = std::min(Lc, n_levels - l0) * nsub;
+  for (int c = 0; c < n_chunks; ++c) {
+    const int l0 = lb[c], units = (lb[c + 1] - lb[c]) * nsub;
     FineChunk fc;
     fc.max_near = *std::max_element(nbound.begin() + (size_t)l0 * nsub, nbound.begin() + (size_t)l0 * nsub + units);
     if (fc.max_near > 65535) // line indices of one unit are 16-bit in the fine kernel's bin table
@@ -500,6 +554,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
 
   // a captured graph replays only the launch plan it was captured with
   std::vector<long long> sig = {Lc, UB, (long long)ctx->alloc_gen};
+  sig.insert(sig.end(), lb.begin(), lb.end());
   for (const FineChunk &fc : fchunks)
     sig.insert(sig.end(), {fc.smem_cap, fc.gstage_cap, fc.block_threads, fc.vsm_rows, fc.resident});
 
@@ -561,8 +616,9 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   cudaEvent_t ev_begin = next_event();
   if (ev_begin) cudaEventRecord(ev_begin, st);
 
-  for (int l0 = 0; l0 < n_levels; l0 += Lc) {
-    const int nl = std::min(Lc, n_levels - l0);
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> copy_marks;
+  for (int c = 0; c < n_chunks; ++c) {
+    const int l0 = lb[c], nl = lb[c + 1] - lb[c];
     PrepParams pp;
     pp.lines = dl;
     pp.tips = ctx->d_tips;
@@ -635,10 +691,10 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     mark(1, e1, e2);
     mark(2, e2, e3);
 
-    const int half = (l0 / Lc) & 1;
+    const int half = c & 1;
     float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p + (size_t)half * Lc * nsub * NT;
     // the half written now was copied out two chunks ago
-    if (host_records && l0 >= 2 * Lc) CK(cudaStreamWaitEvent(st, ctx->rec_copied[half], 0), "wait copy");
+    if (host_records && c >= 2) CK(cudaStreamWaitEvent(st, ctx->rec_copied[half], 0), "wait copy");
     const int out_level0 = o.dev_out ? l0 : 0;
     const int units = nl * nsub;
     // near-line counts of this chunk's units size the fine kernel's staging
@@ -657,14 +713,14 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.err = ctx->d_err;
     fn.phase_clock = nullptr;
     // diagnostics: MARFA_PHASE_CLOCK=<file> records clock64 marks of every
-    // fine-kernel block of the first batch (int64 [units][10]: start, staged, grid 0, grids 1-3, end, near count, grids 4-6, grids 7-9, line-half and site-half cycles) into <file>
+    // fine-kernel block of the first batch (int64 [units][PHASE_SLOTS]) into <file>
     const char *clock_path = std::getenv("MARFA_PHASE_CLOCK");
     if (clock_path && l0 == 0 && !o.graph) {
-      CK(ensure(ctx, ctx->b_count, (size_t)units * 10 * 8), "alloc clock");
-      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * 10 * 8, st), "memset clock");
+      CK(ensure(ctx, ctx->b_count, (size_t)units * PHASE_SLOTS * 8), "alloc clock");
+      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * PHASE_SLOTS * 8, st), "memset clock");
       fn.phase_clock = (long long *)ctx->b_count.p;
     }
-    const FineChunk &fc = fchunks[l0 / Lc];
+    const FineChunk &fc = fchunks[c];
     const int max_near = fc.max_near;
     fn.smem_cap = fc.smem_cap;
     fn.gstage_cap = fc.gstage_cap;
@@ -691,7 +747,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       CK(cudaMemsetAsync(fn.queue, 0, sizeof(int), st), "memset queue");
       CK(launch_fine(fn, run->precision, chi, st), "fine kernel");
       if (fn.phase_clock) {
-        std::vector<long long> pcv((size_t)nu_ * 10);
+        std::vector<long long> pcv((size_t)nu_ * PHASE_SLOTS);
         CK(cudaMemcpyAsync(pcv.data(), fn.phase_clock, pcv.size() * 8, cudaMemcpyDeviceToHost, st), "d2h clock");
         CK(cudaStreamSynchronize(st), "sync clock");
         if (FILE *f = std::fopen(clock_path, "wb")) {
@@ -776,8 +832,12 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     if (host_records) {
       CK(cudaEventRecord(ctx->rec_ready[half], st), "event");
       CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->rec_ready[half], 0), "wait records");
+      cudaEvent_t c0 = next_event(), c1 = next_event();
+      if (c0) cudaEventRecord(c0, ctx->copy_stream);
       CK(cudaMemcpyAsync(o.host_out + (size_t)l0 * nsub * NT, out_base, (size_t)nl * nsub * NT * 4,
                          cudaMemcpyDeviceToHost, ctx->copy_stream), "d2h records");
+      if (c1) cudaEventRecord(c1, ctx->copy_stream);
+      if (c0 && c1) copy_marks.push_back({c0, c1});
       CK(cudaEventRecord(ctx->rec_copied[half], ctx->copy_stream), "event");
     }
     if (o.host_out64)
@@ -801,7 +861,20 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   }
   if (o.dev_out) return MARFA_OK; // asynchronous path: caller synchronises
   CK(cudaStreamSynchronize(st), "stream sync");
-  if (host_records) CK(cudaStreamSynchronize(ctx->copy_stream), "copy stream sync");
+  if (host_records) {
+    CK(cudaStreamSynchronize(ctx->copy_stream), "copy stream sync");
+    // kernel and copy time per level, for the chunks of the next call
+    double kms = 0.0, cms = 0.0;
+    float ms = 0.f;
+    for (auto &m : ctx->marks)
+      if (m.first <= 4 && cudaEventElapsedTime(&ms, m.second.first, m.second.second) == cudaSuccess) kms += ms;
+    for (auto &m : copy_marks)
+      if (cudaEventElapsedTime(&ms, m.first, m.second) == cudaSuccess) cms += ms;
+    if (kms > 0.0 && cms > 0.0 && copy_marks.size() == (size_t)n_chunks) {
+      ctx->rec_compute_ms = kms / n_levels;
+      ctx->rec_copy_ms = cms / n_levels;
+    }
+  }
   int herr = 0;
   CK(cudaMemcpy(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost), "d2h err");
   if (herr) return set_err(ctx, herr, "device reported status %d (isotopologue or temperature outside tables)", herr);

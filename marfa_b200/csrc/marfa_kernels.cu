@@ -966,8 +966,8 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   __syncthreads();
   const int64_t a = sb[0], b = sb[3];
   const int cnt = (int)(b - a);
-  long long *pc = p.phase_clock ? p.phase_clock + (size_t)ub * 10 : nullptr;
-  if (pc && threadIdx.x == 0) { pc[0] = clock64(); pc[5] = cnt; }
+  long long *pc = p.phase_clock ? p.phase_clock + (size_t)ub * PHASE_SLOTS : nullptr;
+  if (pc && threadIdx.x == 0) { pc[0] = clock64(); pc[3] = cnt; }
   // staging area: shared memory, or this block's slice of the global staging buffer
   const bool staged_smem = cnt <= p.smem_cap;
   const int cap = staged_smem ? p.smem_cap : p.gstage_cap;
@@ -1075,7 +1075,6 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   __shared__ unsigned s_touched[(NT + 31) / 32];
   const bool sparse = st.m < p.sparse_lines;
   unsigned *touched = sparse ? s_touched : nullptr;
-  long long t_line = 0, t_site = 0;
   for (int k = 1; k <= 10; ++k) {
     if (sparse) {
       for (int w = threadIdx.x; w < (NT + 31) / 32; w += blockDim.x) s_touched[w] = 0u;
@@ -1119,19 +1118,11 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     }
     __syncthreads();
     if (pc && threadIdx.x == 0) {
-      const long long t2 = clock64();
-      t_line += t1 - t0;
-      t_site += t2 - t1;
-      if (k == 3) pc[3] = t2;
-      if (k == 6) pc[6] = t2;
-      if (k == 9) pc[7] = t2;
+      pc[4 + k] = t1 - t0;
+      pc[14 + k] = clock64() - t1;
     }
   }
-  if (pc && threadIdx.x == 0) {
-    pc[4] = clock64();
-    pc[8] = t_line;
-    pc[9] = t_site;
-  }
+  if (pc && threadIdx.x == 0) pc[4] = clock64();
 }
 
 // Persistent: every block takes units from the work queue until it is empty

@@ -69,6 +69,10 @@ struct FarParams {
 
 // Rows of the fine kernel's slot buffer (values per staged line; the
 // finest-point pass uses 15).
+// diagnostic clock marks per fine-kernel unit: start, staged, grid 0 done,
+// near count, end, line-half cycles of passes 1..10, site-half cycles of
+// passes 1..10
+constexpr int PHASE_SLOTS = 25;
 constexpr int NSLOT = 15;
 
 struct FineParams {
@@ -90,7 +94,7 @@ struct FineParams {
   int gstage_cap;                // lines per block in gstage
   size_t gstage_bytes;           // bytes per block in gstage
   int *err;
-  long long *phase_clock;        // optional [n_units][10] clock64 marks (diagnostics)
+  long long *phase_clock;        // optional [n_units][PHASE_SLOTS] clock64 marks (diagnostics)
   int *queue;                    // work-queue head (zero before the launch)
   const int *order;              // optional processing order of the units
   void *vbuf;                    // per-block slot buffers in global memory

@@ -83,3 +83,26 @@ def test_autotune_keeps_results(gpu):
         big = before > 1e-6 * before.max()
         rel = np.abs(after[big] - before[big]) / before[big]
         assert rel.max() <= tol, (prec, choice, rel.max())
+
+
+def test_host_record_chunks_keep_results(gpu):
+    """Records copied to host memory come in level chunks whose sizes follow
+    the copy/kernel time ratio measured on the previous call; every schedule
+    gives the records of the device-memory path."""
+    torch = pytest.importorskip("torch")
+    tips = read_tips(data_path("TIPS_subset.dat"))
+    w = synth.config(1, 0.03)
+    p = w.profiles[0]
+    P, T, n = (np.asarray(a, dtype=np.float64) for a in (p.pressure, p.temperature, p.density))
+    run = Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule, chi=w.chi,
+              precision="fp32c")
+    with Context(w.lines, tips) as ctx:
+        dev = torch.empty((len(P), run.n_sub, 20481), dtype=torch.float32, device="cuda")
+        ctx.compute_device(run, [len(P)], P, T, n, dev.data_ptr())
+        ctx.synchronize()
+        ref = dev.cpu()
+        for _ in range(3):
+            host = torch.empty_like(ref).pin_memory()
+            ctx.compute(run, P, T, n, out=host)
+            assert torch.equal(host, ref)
+        assert float(ref.abs().sum()) > 0.0
