@@ -34,8 +34,48 @@ struct DevBuf {
 struct Tune {
   int far_chunk = 4096;    // lines per far-kernel block
   int coop_k = 3;          // fine grids whose sites are summed by one warp each
+  int group8_k = 4;        // the next fine grids up to this one: eight lanes per site
   int sparse_lines = 1024; // units with fewer near lines skip untouched sites
   int small_block_lines = 512; // batches whose units all have fewer near lines use small blocks
+};
+
+// Bucket index over the sorted line centres: first[b] = first line with
+// nu >= lo + b w (w = 1 / inv_w, about four lines per bucket), b = 0 .. nb + 1.
+// A search for x only looks between the entries of x's bucket and its
+// neighbours, which hold every lower and upper bound of x whatever the
+// rounding of the bucket position.
+struct NuIndex {
+  double lo = 0.0, inv_w = 0.0;
+  std::vector<int64_t> first;
+  void build(const std::vector<double> &nu) {
+    const int64_t n = (int64_t)nu.size();
+    first.clear();
+    inv_w = 0.0;
+    if (n < 2 || !(nu.back() > nu.front())) return;
+    lo = nu.front();
+    const int64_t nb = std::min<int64_t>(std::max<int64_t>(n / 4, 1), (int64_t)1 << 22);
+    inv_w = (double)nb / (nu.back() - lo);
+    first.resize(nb + 2);
+    int64_t q = 0;
+    for (int64_t b = 0; b <= nb + 1; ++b) {
+      const double edge = lo + (double)b / inv_w;
+      while (q < n && nu[q] < edge) ++q;
+      first[b] = q;
+    }
+  }
+  // lines [a, b) hold the first nu >= x and the first nu > x (or b = n)
+  void range(double x, int64_t n, int64_t &a, int64_t &b) const {
+    if (inv_w == 0.0) {
+      a = 0;
+      b = n;
+      return;
+    }
+    const int64_t nb = (int64_t)first.size() - 2;
+    const double t = (x - lo) * inv_w;
+    const int64_t k = t < 0.0 ? 0 : (t >= (double)nb ? nb : (int64_t)t);
+    a = first[k > 0 ? k - 1 : 0];
+    b = k + 2 <= nb + 1 ? first[k + 2] : n;
+  }
 };
 
 struct marfa_ctx {
@@ -53,6 +93,7 @@ struct marfa_ctx {
   int sm_count = 0;
   int64_t n_lines = 0;
   std::vector<double> nu;  // host copy of the sorted centres (window scan)
+  NuIndex nu_index;        // bucket index over nu (near-line bounds)
   double smax = 0.0;       // largest reference intensity
   double dmin = 0.0, dmax = 0.0;
   int n_iso = 0, n_temp = 0;
@@ -388,6 +429,31 @@ static std::vector<int> level_chunk_sizes(int n, int Lc, bool host_records, doub
   return sz;
 }
 
+// Work-queue order of the units of one batch: most near lines first, ties in
+// unit order (two stable 8-bit radix passes on 65535 - bound; bounds above
+// 65535 are refused later and sort with 65535).
+static void order_by_bound(const int *nb, int n, int *out, std::vector<int> &tmp) {
+  tmp.resize(n);
+  auto key = [&](int i) { return 65535 - std::min(std::max(nb[i], 0), 65535); };
+  int cnt[256];
+  std::fill(cnt, cnt + 256, 0);
+  for (int i = 0; i < n; ++i) ++cnt[key(i) & 255];
+  for (int d = 0, sum = 0; d < 256; ++d) {
+    const int c = cnt[d];
+    cnt[d] = sum;
+    sum += c;
+  }
+  for (int i = 0; i < n; ++i) tmp[cnt[key(i) & 255]++] = i;
+  std::fill(cnt, cnt + 256, 0);
+  for (int i = 0; i < n; ++i) ++cnt[key(i) >> 8];
+  for (int d = 0, sum = 0; d < 256; ++d) {
+    const int c = cnt[d];
+    cnt[d] = sum;
+    sum += c;
+  }
+  for (int i = 0; i < n; ++i) out[cnt[key(tmp[i]) >> 8]++] = tmp[i];
+}
+
 // The whole computation for a flat list of levels.
 int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *P,
                const double *T, const double *dens, const Outputs &o, cudaStream_t st) {
@@ -506,22 +572,23 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   // queue (most lines first) before anything is launched, so that no call
   // waits for the device in the middle of its launches.
   std::vector<int> nbound((size_t)n_levels * nsub), order_all((size_t)n_levels * nsub);
+  const double *nu = ctx->nu.data();
   for (int l = 0; l < n_levels; ++l)
     for (int isub = 0; isub < nsub; ++isub) {
       const double lo = pl.s[isub] - 1.0 - std::max(ctx->dmax, 0.0) * P[l] - 1e-6;
       const double hi = pl.s[isub] + DELTA_WV + 1.0 - std::min(ctx->dmin, 0.0) * P[l] + 1e-6;
-      const auto a0 = std::lower_bound(ctx->nu.begin(), ctx->nu.end(), lo);
-      const auto b0 = std::upper_bound(a0, ctx->nu.end(), hi);
+      int64_t a, b;
+      ctx->nu_index.range(lo, N, a, b);
+      const int64_t a0 = std::lower_bound(nu + a, nu + b, lo) - nu;
+      ctx->nu_index.range(hi, N, a, b);
+      const int64_t b0 = std::upper_bound(nu + std::max(a, a0), nu + std::max(b, a0), hi) - nu;
       nbound[(size_t)l * nsub + isub] = (int)(b0 - a0);
     }
+  std::vector<int> tmp;
   for (int c = 0; c < n_chunks; ++c) {
     const int base = lb[c] * nsub, units = (lb[c + 1] - lb[c]) * nsub;
-    for (int u0 = 0; u0 < units; u0 += UB) {
-      const int nu_ = std::min(UB, units - u0);
-      int *o_ = order_all.data() + base + u0;
-      for (int i = 0; i < nu_; ++i) o_[i] = i;
-      std::stable_sort(o_, o_ + nu_, [&](int x, int y) { return nbound[base + u0 + x] > nbound[base + u0 + y]; });
-    }
+    for (int u0 = 0; u0 < units; u0 += UB)
+      order_by_bound(nbound.data() + base + u0, std::min(UB, units - u0), order_all.data() + base + u0, tmp);
   }
   CK(ensure(ctx, ctx->b_order, order_all.size() * 4), "alloc order");
 
@@ -734,6 +801,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.vbuf = ctx->b_vbuf.p;
     fn.queue = (int *)ctx->b_queue.p;
     fn.coop_k = ctx->tune.coop_k;
+    fn.group8_k = ctx->tune.group8_k;
     fn.sparse_lines = ctx->tune.sparse_lines;
     const int UBc = UB;
     for (int u0 = 0; u0 < units; u0 += UBc) {
@@ -975,6 +1043,7 @@ int marfa_ctx_create(const marfa_line_record *lines, int64_t n_lines, const doub
     ctx->dmin = std::min(ctx->dmin, (double)r.delta_air);
     ctx->dmax = std::max(ctx->dmax, (double)r.delta_air);
   }
+  ctx->nu_index.build(ctx->nu);
   int rc = MARFA_OK;
   auto fail = [&](cudaError_t e, const char *w) {
     rc = cuda_fail(ctx, e, w);

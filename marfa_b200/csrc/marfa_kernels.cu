@@ -299,7 +299,13 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
         } else {
           int kb[3];
 #pragma unroll
-          for (int j = 0; j < 3; ++j) kb[j] = j < pc.nb ? first_k_past(D, pc.b[j], pc.strict[j]) : NFAR;
+          for (int j = 0; j < 3; ++j) {
+            // positions D .. D + 10: a boundary outside that span (with a
+            // margin far above the rounding of D) needs no search
+            const double bj = pc.b[j];
+            kb[j] = j >= pc.nb || D + 10.0 < bj - 1e-6 ? NFAR
+                  : (D > bj + 1e-6 ? 0 : first_k_past(D, bj, pc.strict[j]));
+          }
           float F[NFAR];
           if (kb[0] == 0 && kb[1] == NFAR) { // one chi piece over the whole line
             // chi(d + k/2) = chi(d) * 2^(r/2)^k: one exponential per line, the
@@ -510,12 +516,12 @@ __device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Lane
   }
 }
 
-// Sum over the lanes of a warp (lane 0 gets the total) when `coop`.
-__device__ __forceinline__ double coop_sum(double v, bool coop) {
-  if (coop) {
+// Sum over each group of G lanes (G = 1, 2, 4, 8, 16 or 32; the first lane
+// of the group gets the total).  Every lane of the warp takes part.
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-  }
+  for (int off = G >> 1; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off, G);
   return v;
 }
 
@@ -588,6 +594,37 @@ struct LineEval {
     E6 = horner<Real>(Y, 5.0, 13.3988, 1.49645);
   }
 
+  // Region 4 (VY < 0.02, 1 < VX, VX + VY < 5.5) as voigt_eval computes it:
+  // the Lorentz asymptote beyond VX = 5 (Spectroscopy.f90:232-241), the
+  // Doppler core plus the tabulated Lorentz wing beyond sqrt(14)
+  // (Spectroscopy.f90:243-261), else the Doppler core.  Inline, so that the
+  // passes of the upper levels (where this region is frequent) make no call.
+  __device__ __forceinline__ Real region4(double ax, double VXd, const LevelConst &lv, double sqrt14) const {
+    const Real axr = (Real)ax;
+    const Real VX = (Real)VXd, VXs = VX * VX;
+    if (VXd > 5.0) {
+      const Real lor = fast_div(lorA, axr * axr + g2);
+      Real chi = (Real)1;
+      if (CHI != CHI_NONE)
+        chi = (sizeof(Real) == 8) ? (Real)chi_factor_d<CHI>(ax, lv) : (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
+      return lor * chi * ((Real)1. + (Real)1.5 / VXs);
+    }
+    const Real dop = hum * exp_neg(VXs);
+    if (VXd > sqrt14) {
+      int I = (int)(VXd / 0.5 - 1.00001); // 1-based, truncation
+      I = I < 1 ? 1 : (I > 8 ? 8 : I);
+      // nodes U_i = 1 + i / 2 and weights W_i, i = 0 .. 8
+      auto W = [](int i) {
+        return i == 0 ? -0.688 : i == 1 ? 0.2667 : i == 2 ? 0.6338 : i == 3 ? 0.4405 : i == 4 ? 0.2529
+             : i == 5 ? 0.1601 : i == 6 ? 0.1131 : i == 7 ? 0.0853 : 0.068;
+      };
+      const double u0 = 1.0 + 0.5 * (double)(I - 1), u1 = 1.0 + 0.5 * (double)I;
+      const Real F = (Real)(2. * (W(I - 1) * (u1 - VXd) + W(I) * (VXd - u0)));
+      return dop + lorA / (axr * axr) * ((Real)1. + F);
+    }
+    return dop;
+  }
+
   __device__ __forceinline__ Real operator()(double X, const LevelConst &lv, double sqrt14) const {
     const double ax = fabs(X);
     if (qx < 0.0) return vy < 0.0 ? (Real)1 : (Real)ax; // diagnostic shapes
@@ -601,8 +638,7 @@ struct LineEval {
     }
     const double sum = VXd + vy;
     const bool r1 = sum >= 15.0, r2 = !r1 && sum >= 5.5;
-    if (!r1 && !r2 && !(VXd <= 1.0 || vy >= 0.02))
-      return voigt_core<Real, CHI>(X, qx, vy, lorA, g2, hum, lv.perrin_b1, lv.perrin_b2, sqrt14);
+    if (!r1 && !r2 && !(VXd <= 1.0 || vy >= 0.02)) return region4(ax, VXd, lv, sqrt14);
     const Real VX = (Real)VXd;
     const Real x = VX * VX;
     const Real z = (Real)0, o = (Real)1;
@@ -635,7 +671,11 @@ __device__ __forceinline__ double i2d(int n) {
 template <bool F64, int CHI>
 __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearStore<F64>::Real *vb, int cap,
                           unsigned *touched) {
-  LineEval<F64, CHI> ev;
+  // Every offset of the line half is below 3 cm-1 in magnitude (at most
+  // 4.5 H_k for centre lines, 2 H_{k-1} for near lines, k >= 1), where each
+  // chi factor is exactly 1 (ChiFactors.f90: the factors start at |X| = 3):
+  // the shape is evaluated without one.
+  LineEval<F64, CHI_NONE> ev;
   const double UU = st.uu[q];
   const int cls = q < st.c0 ? 0 : (q < st.c1 ? 1 : 2);
   // value of slot `slot` at offset X; `site` is marked as touched when the
@@ -769,13 +809,17 @@ constexpr int GB = 2;
 // mid e.  The mid takes exactly the lines that give L(e) (its walk conditions
 // are those of L(e), at offset X + H_{k+1}), so one pass over the edge's line
 // runs serves all three accumulators.  Lanes of a warp stride over the lines
-// when stride > 1 (lane 0 stores the warp sums).
-template <bool F64>
+// when stride > 1: a group of `stride` lanes (aligned within the warp) sums
+// one cell and its first lane stores the sums.  Every lane of the warp calls
+// this the same number of times (the group sum shuffles); a group whose cell
+// lies past the grid (e > ntk) takes no lines and stores nothing.
+template <bool F64, int stride>
 __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typename NearStore<F64>::Real *vb,
-                            int cap, void *scr, int lane, int stride) {
+                            int cap, void *scr, int lane) {
   using Real = typename NearStore<F64>::Real;
   const double hk = h_k(k), hk1 = h_k(k - 1);
   const int ntk = nt_k(k), sh = 11 - k;
+  const bool valid = e <= ntk;
   const bool hasL = e >= 1, hasP = e <= ntk - 1; // hasL is also "has M"
   const int wl = 2 * ((e + 1) / 2) + 2, wp = 2 * ((e + 2) / 2) + 2; // walk ends of e, e+1 in bins
   Acc<F64> aL, aP, aM;
@@ -795,7 +839,7 @@ __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typena
     }
   };
   { // left walk: bins e+1 .. e+3
-    const int q0 = st.lbL(k, e + 1), q1 = st.lbL(k, e + 4);
+    const int q0 = valid ? st.lbL(k, e + 1) : 0, q1 = valid ? st.lbL(k, e + 4) : 0;
     for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
 #pragma unroll
       for (int j = 0; j < GB; ++j) {
@@ -812,7 +856,7 @@ __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typena
   { // right walk: V bins ntk-e+1 .. ntk-e+3
     const int rL = ntk + 1 - e, rP = ntk - e;
     const int wrl = 2 * ((rL + 1) / 2) + 2, wrp = 2 * ((rP + 1) / 2) + 2;
-    const int q0 = st.lbV(k, ntk - e + 4), q1 = st.lbV(k, ntk - e + 1);
+    const int q0 = valid ? st.lbV(k, ntk - e + 4) : 0, q1 = valid ? st.lbV(k, ntk - e + 1) : 0;
     for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
 #pragma unroll
       for (int j = 0; j < GB; ++j) {
@@ -826,7 +870,7 @@ __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typena
       flush();
     }
   }
-  if (e <= 2) { // near-left lines with D < H_{k-1}
+  if (valid && e <= 2) { // near-left lines with D < H_{k-1}
     const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
     for (int qb = q0 + lane; qb < st.c0; qb += GB * stride) {
 #pragma unroll
@@ -842,7 +886,7 @@ __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typena
       flush();
     }
   }
-  if (e >= ntk - 2) { // near-right lines with U < H_{k-1}
+  if (valid && e >= ntk - 2) { // near-right lines with U < H_{k-1}
     const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
     for (int qb = st.c1 + lane; qb < q1; qb += GB * stride) {
 #pragma unroll
@@ -858,10 +902,9 @@ __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typena
       flush();
     }
   }
-  const bool coop = stride > 1;
-  const double vL = coop_sum(aL.value(), coop), vP = coop_sum(aP.value(), coop);
-  const double vM = coop_sum(aM.value(), coop);
-  if (lane == 0) {
+  const double vL = group_sum<stride>(aL.value()), vP = group_sum<stride>(aP.value());
+  const double vM = group_sum<stride>(aM.value());
+  if (valid && lane == 0) {
     Real *o = (Real *)scr;
     const int cb = base_k(k) - NT0;
     if (hasL) {
@@ -1089,22 +1132,29 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     const long long t1 = pc ? clock64() : 0;
     if (k <= 9) {
       const int ntk = nt_k(k), nsite = ntk + 1, cb = base_k(k) - NT0;
-      const bool coop = k <= p.coop_k && !sparse; // few lines per site in sparse units
-      const int lane = coop ? (threadIdx.x & 31) : 0;
-      const int first = coop ? warp_id() : threadIdx.x, step = coop ? (blockDim.x >> 5) : blockDim.x;
-      for (int e = first; e < nsite; e += step) {
-        if (sparse && !is_touched(s_touched, e)) { // no contribution: zero accumulators
-          if (lane == 0) {
+      // lanes per cell: a warp on the coarsest grids, groups of 8 on the
+      // next ones, one thread on the dense grids and in sparse units (few
+      // lines per site)
+      const int G = sparse ? 1 : (k <= p.coop_k ? 32 : (k <= p.group8_k ? 8 : 1));
+      if (G == 1) {
+        for (int e = threadIdx.x; e < nsite; e += blockDim.x) {
+          if (sparse && !is_touched(s_touched, e)) { // no contribution: zero accumulators
             if (e >= 1) {
               scr[SCR_FINE_L + cb + e - 1] = (Real)0;
               scr[SCR_FINE_M + cb + e - 1] = (Real)0;
             }
             if (e <= ntk - 1) scr[SCR_FINE_P + cb + e] = (Real)0;
+            continue;
           }
-          continue;
+          gather_cell<F64, 1>(st, k, e, vb, vcap, scr, 0);
         }
-        if (coop) gather_cell<F64>(st, k, e, vb, vcap, scr, lane, 32);
-        else gather_cell<F64>(st, k, e, vb, vcap, scr, 0, 1);
+      } else {
+        const int lane = threadIdx.x & (G - 1), grp = threadIdx.x / G, ngrp = blockDim.x / G;
+        const int rounds = (nsite + ngrp - 1) / ngrp; // the same for every lane
+        for (int r = 0; r < rounds; ++r) {
+          if (G == 32) gather_cell<F64, 32>(st, k, grp + r * ngrp, vb, vcap, scr, lane);
+          else gather_cell<F64, 8>(st, k, grp + r * ngrp, vb, vcap, scr, lane);
+        }
       }
     } else {
       for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) {
