@@ -91,6 +91,12 @@ struct marfa_ctx {
   // (ms), which shape the level chunks of the next such call
   double rec_compute_ms = 0.0, rec_copy_ms = 0.0;
   int sm_count = 0;
+  // second stream and buffer set: with host records, consecutive chunks run
+  // on alternating streams with their own line and scratch buffers, so that
+  // one chunk's first kernels fill the SMs the previous chunk's last
+  // kernels leave idle
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int64_t n_lines = 0;
   std::vector<double> nu;  // host copy of the sorted centres (window scan)
   NuIndex nu_index;        // bucket index over nu (near-line bounds)
@@ -108,6 +114,7 @@ struct marfa_ctx {
   // grow-only work buffers
   DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
       b_out, b_out64, b_dump, b_count, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order, b_tune;
+  DevBuf b2_nus, b2_gen, b2_hot, b2_rank, b2_snu, b2_sidx, b2_far, b2_scr, b2_gstage, b2_vbuf, b2_queue;
   std::string err;
   // pinned staging of the per-call host tables (see Staging)
   void *pinned = nullptr;
@@ -505,6 +512,11 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   // host records: at least four chunks of levels, so that the copy of each
   // overlaps the computation of the next
   const bool host_records = o.host_out != nullptr && !adj;
+  const bool two = host_records && !o.host_out64 && !o.host_dump && !o.graph && n_levels >= 2;
+  if (two) { // two buffer sets in the same memory
+    Lc = std::max(1, Lc / 2);
+    UB = std::max(1, UB / 2);
+  }
   if (host_records && !ctx->sm_count)
     CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device), "device attribute");
   // chunk boundaries: chunk c holds levels [lb[c], lb[c + 1])
@@ -523,6 +535,11 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       if (!ctx->rec_copied[h]) CK(cudaEventCreateWithFlags(&ctx->rec_copied[h], cudaEventDisableTiming), "event");
     }
   }
+  if (two) {
+    if (!ctx->stream2) CK(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking), "second stream");
+    if (!ctx->fork_ev) CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming), "event");
+    if (!ctx->join_ev) CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming), "event");
+  }
 
   CK(ensure(ctx, ctx->b_nus, (size_t)Lc * N * 8), "alloc nus");
   CK(ensure(ctx, ctx->b_gen, (size_t)Lc * N * sizeof(LineGen)), "alloc gen");
@@ -532,6 +549,16 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   CK(ensure(ctx, ctx->b_sidx, (size_t)Lc * N * 4), "alloc sidx");
   CK(ensure(ctx, ctx->b_far, (size_t)Lc * std::max(C, 1) * NFAR * 8), "alloc far");
   CK(ensure(ctx, ctx->b_scr, (size_t)UB * SCR_STRIDE * elem), "alloc scratch");
+  if (two) {
+    CK(ensure(ctx, ctx->b2_nus, ctx->b_nus.cap), "alloc nus");
+    CK(ensure(ctx, ctx->b2_gen, ctx->b_gen.cap), "alloc gen");
+    CK(ensure(ctx, ctx->b2_hot, ctx->b_hot.cap), "alloc hot");
+    CK(ensure(ctx, ctx->b2_rank, ctx->b_rank.cap), "alloc rank");
+    CK(ensure(ctx, ctx->b2_snu, ctx->b_snu.cap), "alloc snu");
+    CK(ensure(ctx, ctx->b2_sidx, ctx->b_sidx.cap), "alloc sidx");
+    CK(ensure(ctx, ctx->b2_far, ctx->b_far.cap), "alloc far");
+    CK(ensure(ctx, ctx->b2_scr, ctx->b_scr.cap), "alloc scratch");
+  }
   if (adj) {
     CK(ensure(ctx, ctx->b_gscr, (size_t)UB * SCR_STRIDE * 8), "alloc gradient scratch");
     CK(ensure(ctx, ctx->b_aux, (size_t)Lc * N * sizeof(LineAux)), "alloc line partials");
@@ -618,6 +645,11 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   if (gstage_need) CK(ensure(ctx, ctx->b_gstage, gstage_need), "alloc staging");
   CK(ensure(ctx, ctx->b_vbuf, vbuf_need), "alloc slot buffers");
   CK(ensure(ctx, ctx->b_queue, 256), "alloc queue");
+  if (two) {
+    if (gstage_need) CK(ensure(ctx, ctx->b2_gstage, gstage_need), "alloc staging");
+    CK(ensure(ctx, ctx->b2_vbuf, vbuf_need), "alloc slot buffers");
+    CK(ensure(ctx, ctx->b2_queue, 256), "alloc queue");
+  }
 
   // a captured graph replays only the launch plan it was captured with
   std::vector<long long> sig = {Lc, UB, (long long)ctx->alloc_gen};
@@ -684,8 +716,25 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   if (ev_begin) cudaEventRecord(ev_begin, st);
 
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> copy_marks;
+  struct ChunkBufs {
+    DevBuf *nus, *gen, *hot, *rank, *snu, *sidx, *far, *scr, *gstage, *vbuf, *queue;
+  };
+  const ChunkBufs sets[2] = {
+      {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far, &ctx->b_scr,
+       &ctx->b_gstage, &ctx->b_vbuf, &ctx->b_queue},
+      {&ctx->b2_nus, &ctx->b2_gen, &ctx->b2_hot, &ctx->b2_rank, &ctx->b2_snu, &ctx->b2_sidx, &ctx->b2_far,
+       &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue}};
+  if (two) { // the second stream starts after the tables and the error flag
+    CK(cudaEventRecord(ctx->fork_ev, st), "event");
+    CK(cudaStreamWaitEvent(ctx->stream2, ctx->fork_ev, 0), "fork");
+  }
   for (int c = 0; c < n_chunks; ++c) {
     const int l0 = lb[c], nl = lb[c + 1] - lb[c];
+    // chunk c runs on stream c % 2 with buffer set c % 2 (one of each
+    // without host records); chunk c - 2 used the same ones on the same stream
+    const int set = two ? (c & 1) : 0;
+    const ChunkBufs &B = sets[set];
+    cudaStream_t cs = set ? ctx->stream2 : st;
     PrepParams pp;
     pp.lines = dl;
     pp.tips = ctx->d_tips;
@@ -695,14 +744,14 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     pp.n_levels = nl;
     pp.c = cst;
     pp.sscale = sscale;
-    pp.nus = (double *)ctx->b_nus.p;
-    pp.gen = (LineGen *)ctx->b_gen.p;
-    pp.hot32 = f64 ? nullptr : (Hot32 *)ctx->b_hot.p;
-    pp.hot64 = f64 ? (Hot64 *)ctx->b_hot.p : nullptr;
+    pp.nus = (double *)B.nus->p;
+    pp.gen = (LineGen *)B.gen->p;
+    pp.hot32 = f64 ? nullptr : (Hot32 *)B.hot->p;
+    pp.hot64 = f64 ? (Hot64 *)B.hot->p : nullptr;
     pp.err = ctx->d_err;
     cudaEvent_t e0 = next_event(), e1 = next_event(), e2 = next_event(), e3 = next_event();
-    if (e0) cudaEventRecord(e0, st);
-    CK(launch_prep(pp, st), "prep kernel");
+    if (e0) cudaEventRecord(e0, cs);
+    CK(launch_prep(pp, cs), "prep kernel");
     ctx->launches += 1;
     if (adj) {
       AdjPrepParams ap;
@@ -714,22 +763,22 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       ap.n_levels = nl;
       ap.c = cst;
       ap.aux = (LineAux *)ctx->b_aux.p;
-      CK(launch_adjoint_prep(ap, st), "adjoint prep kernel");
+      CK(launch_adjoint_prep(ap, cs), "adjoint prep kernel");
       ctx->launches += 1;
     }
-    if (e1) cudaEventRecord(e1, st);
+    if (e1) cudaEventRecord(e1, cs);
     SortParams sp;
     sp.nu = ctx->d_nu;
     sp.nus = pp.nus;
     sp.margin = d_margin + l0;
     sp.n = N;
     sp.n_levels = nl;
-    sp.rank = (int64_t *)ctx->b_rank.p;
-    sp.snu = (double *)ctx->b_snu.p;
-    sp.sidx = (int *)ctx->b_sidx.p;
-    CK(launch_sort(sp, st), "sort kernels");
+    sp.rank = (int64_t *)B.rank->p;
+    sp.snu = (double *)B.snu->p;
+    sp.sidx = (int *)B.sidx->p;
+    CK(launch_sort(sp, cs), "sort kernels");
     ctx->launches += 2;
-    if (e2) cudaEventRecord(e2, st);
+    if (e2) cudaEventRecord(e2, cs);
     FarParams fp;
     fp.nus = pp.nus;
     fp.hot32 = pp.hot32;
@@ -747,13 +796,13 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fp.sscale = sscale;
     fp.shape = run->shape;
     fp.c = cst;
-    fp.out = (double *)ctx->b_far.p;
-    CK(launch_far(fp, run->precision, chi, st), "far kernel");
+    fp.out = (double *)B.far->p;
+    CK(launch_far(fp, run->precision, chi, cs), "far kernel");
     if (C > 0) {
       ctx->launches += 1;
       ctx->far_launches += 1;
     }
-    if (e3) cudaEventRecord(e3, st);
+    if (e3) cudaEventRecord(e3, cs);
     mark(0, e0, e1);
     mark(1, e1, e2);
     mark(2, e2, e3);
@@ -761,7 +810,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     const int half = c & 1;
     float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p + (size_t)half * Lc * nsub * NT;
     // the half written now was copied out two chunks ago
-    if (host_records && c >= 2) CK(cudaStreamWaitEvent(st, ctx->rec_copied[half], 0), "wait copy");
+    if (host_records && c >= 2) CK(cudaStreamWaitEvent(cs, ctx->rec_copied[half], 0), "wait copy");
     const int out_level0 = o.dev_out ? l0 : 0;
     const int units = nl * nsub;
     // near-line counts of this chunk's units size the fine kernel's staging
@@ -776,7 +825,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.sscale = sscale;
     fn.shape = run->shape;
     fn.c = cst;
-    fn.scratch = ctx->b_scr.p;
+    fn.scratch = B.scr->p;
     fn.err = ctx->d_err;
     fn.phase_clock = nullptr;
     // diagnostics: MARFA_PHASE_CLOCK=<file> records clock64 marks of every
@@ -784,7 +833,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     const char *clock_path = std::getenv("MARFA_PHASE_CLOCK");
     if (clock_path && l0 == 0 && !o.graph) {
       CK(ensure(ctx, ctx->b_count, (size_t)units * PHASE_SLOTS * 8), "alloc clock");
-      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * PHASE_SLOTS * 8, st), "memset clock");
+      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * PHASE_SLOTS * 8, cs), "memset clock");
       fn.phase_clock = (long long *)ctx->b_count.p;
     }
     const FineChunk &fc = fchunks[c];
@@ -792,14 +841,14 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.smem_cap = fc.smem_cap;
     fn.gstage_cap = fc.gstage_cap;
     fn.gstage_bytes = fc.gstage_bytes;
-    fn.gstage = fc.gstage_cap ? ctx->b_gstage.p : nullptr;
+    fn.gstage = fc.gstage_cap ? B.gstage->p : nullptr;
     fn.block_threads = fc.block_threads;
     fn.vsm_rows = fc.vsm_rows;
     const int resident = fc.resident;
     fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
     fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
-    fn.vbuf = ctx->b_vbuf.p;
-    fn.queue = (int *)ctx->b_queue.p;
+    fn.vbuf = B.vbuf->p;
+    fn.queue = (int *)B.queue->p;
     fn.coop_k = ctx->tune.coop_k;
     fn.group8_k = ctx->tune.group8_k;
     fn.sparse_lines = ctx->tune.sparse_lines;
@@ -811,13 +860,13 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       fn.order = (const int *)ctx->b_order.p + (size_t)l0 * nsub + u0;
       fn.grid = std::min(resident, nu_);
       cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
-      if (f0) cudaEventRecord(f0, st);
-      CK(cudaMemsetAsync(fn.queue, 0, sizeof(int), st), "memset queue");
-      CK(launch_fine(fn, run->precision, chi, st), "fine kernel");
+      if (f0) cudaEventRecord(f0, cs);
+      CK(cudaMemsetAsync(fn.queue, 0, sizeof(int), cs), "memset queue");
+      CK(launch_fine(fn, run->precision, chi, cs), "fine kernel");
       if (fn.phase_clock) {
         std::vector<long long> pcv((size_t)nu_ * PHASE_SLOTS);
-        CK(cudaMemcpyAsync(pcv.data(), fn.phase_clock, pcv.size() * 8, cudaMemcpyDeviceToHost, st), "d2h clock");
-        CK(cudaStreamSynchronize(st), "sync clock");
+        CK(cudaMemcpyAsync(pcv.data(), fn.phase_clock, pcv.size() * 8, cudaMemcpyDeviceToHost, cs), "d2h clock");
+        CK(cudaStreamSynchronize(cs), "sync clock");
         if (FILE *f = std::fopen(clock_path, "wb")) {
           std::fwrite(pcv.data(), 8, pcv.size(), f);
           std::fclose(f);
@@ -825,10 +874,10 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
         fn.phase_clock = nullptr;
       }
       ctx->launches += 1;
-      if (f1) cudaEventRecord(f1, st);
+      if (f1) cudaEventRecord(f1, cs);
       if (adj) {
         CascadeAdjParams ca;
-        ca.scratch = (const double *)ctx->b_scr.p;
+        ca.scratch = (const double *)B.scr->p;
         ca.far = fp.out;
         ca.sub_chunk0 = d_sc0;
         ca.lv = pp.lv;
@@ -840,7 +889,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
         ca.target = run->target;
         ca.cot = o.vjp->cot;
         ca.gscratch = (double *)ctx->b_gscr.p;
-        CK(launch_cascade_adjoint(ca, st), "cascade adjoint kernel");
+        CK(launch_cascade_adjoint(ca, cs), "cascade adjoint kernel");
         AdjointParams ad;
         ad.snu = sp.snu;
         ad.sidx = sp.sidx;
@@ -864,15 +913,15 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
         ad.dgair = o.vjp->dgair;
         ad.dT = o.vjp->dT;
         ad.dP = o.vjp->dP;
-        CK(launch_line_adjoint(ad, chi, std::min(64, (max_near + 255) / 256), st), "line adjoint kernels");
+        CK(launch_line_adjoint(ad, chi, std::min(64, (max_near + 255) / 256), cs), "line adjoint kernels");
         ctx->launches += 2 + (pl.max_chunks > 0 ? 1 : 0);
-        if (f2) cudaEventRecord(f2, st);
+        if (f2) cudaEventRecord(f2, cs);
         mark(3, f0, f1);
         mark(4, f1, f2);
         continue;
       }
       CascadeParams cp;
-      cp.scratch = ctx->b_scr.p;
+      cp.scratch = B.scr->p;
       cp.far = fp.out;
       cp.sub_chunk0 = d_sc0;
       cp.lv = pp.lv;
@@ -891,14 +940,14 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
         cp.dump = (double *)ctx->b_dump.p;
         cp.dump_unit = (o.dump_level - l0) * nsub + o.dump_sub;
       }
-      CK(launch_cascade(cp, run->precision, st), "cascade kernel");
+      CK(launch_cascade(cp, run->precision, cs), "cascade kernel");
       ctx->launches += cp.dump ? 2 : 1;
-      if (f2) cudaEventRecord(f2, st);
+      if (f2) cudaEventRecord(f2, cs);
       mark(3, f0, f1);
       mark(4, f1, f2);
     }
     if (host_records) {
-      CK(cudaEventRecord(ctx->rec_ready[half], st), "event");
+      CK(cudaEventRecord(ctx->rec_ready[half], cs), "event");
       CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->rec_ready[half], 0), "wait records");
       cudaEvent_t c0 = next_event(), c1 = next_event();
       if (c0) cudaEventRecord(c0, ctx->copy_stream);
@@ -910,7 +959,11 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     }
     if (o.host_out64)
       CK(cudaMemcpyAsync(o.host_out64 + (size_t)l0 * nsub * NT, ctx->b_out64.p, (size_t)nl * nsub * NT * 8,
-                         cudaMemcpyDeviceToHost, st), "d2h records64");
+                         cudaMemcpyDeviceToHost, cs), "d2h records64");
+  }
+  if (two) { // join the second stream
+    CK(cudaEventRecord(ctx->join_ev, ctx->stream2), "event");
+    CK(cudaStreamWaitEvent(st, ctx->join_ev, 0), "join");
   }
   cudaEvent_t ev_end = next_event();
   if (ev_end) cudaEventRecord(ev_end, st);
@@ -1079,6 +1132,7 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
   void *ps[] = {ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta,
                 ctx->d_iso, ctx->d_tips, ctx->d_err, ctx->d_S64, ctx->d_gair64};
   for (void *p : ps)
@@ -1086,7 +1140,9 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
   DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
                   &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
                   &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_gstage, &ctx->b_aux,
-                  &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order, &ctx->b_tune};
+                  &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order, &ctx->b_tune,
+                  &ctx->b2_nus, &ctx->b2_gen, &ctx->b2_hot, &ctx->b2_rank, &ctx->b2_snu, &ctx->b2_sidx,
+                  &ctx->b2_far, &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue};
   for (DevBuf *b : bs) release(*b);
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
@@ -1099,6 +1155,9 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
+  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
