@@ -116,11 +116,14 @@ struct marfa_ctx {
       b_out, b_out64, b_dump, b_count, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order, b_tune;
   DevBuf b2_nus, b2_gen, b2_hot, b2_rank, b2_snu, b2_sidx, b2_far, b2_scr, b2_gstage, b2_vbuf, b2_queue;
   std::string err;
-  // pinned staging of the per-call host tables (see Staging)
-  void *pinned = nullptr;
-  size_t pinned_cap = 0;
-  cudaEvent_t pinned_ev = nullptr;
-  bool pinned_pending = false;
+  // pinned staging of the per-call host tables (see Staging): a ring of
+  // buffers, used by consecutive calls in turn
+  static constexpr int NPIN = 4;
+  void *pinned[NPIN] = {};
+  size_t pinned_cap[NPIN] = {};
+  cudaEvent_t pinned_ev[NPIN] = {};
+  bool pinned_pending[NPIN] = {};
+  int pinned_next = 0;
   std::vector<cudaEvent_t> events;
   // timing marks of the last compute call: (family, start, stop); family 5
   // is the whole call
@@ -183,41 +186,49 @@ void release(DevBuf &b) {
 namespace {
 
 // The host tables of one call (windows, chunks, levels, work order) reach the
-// device through one pinned buffer of the context: a copy from pageable memory
+// device through a pinned buffer of the context: a copy from pageable memory
 // would first wait for the stream to drain, so that the host planning of a
-// call could not overlap the kernels of the previous one.  The buffer is
-// rewritten only after the copies of the previous call have completed.
+// call could not overlap the kernels of the previous one.  Consecutive calls
+// take the buffers of a ring in turn, and a buffer is rewritten only after
+// its previous copies have completed, so that the host can queue calls up to
+// the ring's length ahead of the device (and a late host thread does not
+// leave the device idle).
 struct Staging {
   marfa_ctx *ctx;
   cudaStream_t st;
   size_t off = 0;
+  int slot = 0;
   cudaError_t begin(size_t bytes) {
     cudaError_t e = cudaSuccess;
-    if (ctx->pinned_pending) {
-      if ((e = cudaEventSynchronize(ctx->pinned_ev))) return e;
-      ctx->pinned_pending = false;
+    slot = ctx->pinned_next;
+    ctx->pinned_next = (slot + 1) % marfa_ctx::NPIN;
+    if (ctx->pinned_pending[slot]) {
+      if ((e = cudaEventSynchronize(ctx->pinned_ev[slot]))) return e;
+      ctx->pinned_pending[slot] = false;
     }
-    if (!ctx->pinned_ev && (e = cudaEventCreateWithFlags(&ctx->pinned_ev, cudaEventDisableTiming))) return e;
-    if (bytes > ctx->pinned_cap) {
-      if (ctx->pinned) cudaFreeHost(ctx->pinned);
-      ctx->pinned = nullptr;
-      ctx->pinned_cap = 0;
-      if ((e = cudaMallocHost(&ctx->pinned, bytes))) return e;
-      ctx->pinned_cap = bytes;
+    if (!ctx->pinned_ev[slot] &&
+        (e = cudaEventCreateWithFlags(&ctx->pinned_ev[slot], cudaEventDisableTiming)))
+      return e;
+    if (bytes > ctx->pinned_cap[slot]) {
+      if (ctx->pinned[slot]) cudaFreeHost(ctx->pinned[slot]);
+      ctx->pinned[slot] = nullptr;
+      ctx->pinned_cap[slot] = 0;
+      if ((e = cudaMallocHost(&ctx->pinned[slot], bytes))) return e;
+      ctx->pinned_cap[slot] = bytes;
     }
     off = 0;
     return e;
   }
   cudaError_t put(void *dst, const void *src, size_t bytes) {
     if (bytes == 0) return cudaSuccess;
-    char *h = (char *)ctx->pinned + off;
+    char *h = (char *)ctx->pinned[slot] + off;
     std::memcpy(h, src, bytes);
     off += (bytes + 15) & ~(size_t)15;
     return cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, st);
   }
   cudaError_t end() {
-    cudaError_t e = cudaEventRecord(ctx->pinned_ev, st);
-    if (e == cudaSuccess) ctx->pinned_pending = true;
+    cudaError_t e = cudaEventRecord(ctx->pinned_ev[slot], st);
+    if (e == cudaSuccess) ctx->pinned_pending[slot] = true;
     return e;
   }
   static size_t room(size_t bytes) { return (bytes + 15) & ~(size_t)15; }
@@ -598,19 +609,23 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   // dmin P).  The bound sizes the fine kernel's staging and orders its work
   // queue (most lines first) before anything is launched, so that no call
   // waits for the device in the middle of its launches.
+  // The bound of a chunk's units uses the chunk's largest pressure (the
+  // widest shift range): one count per subinterval and chunk.
   std::vector<int> nbound((size_t)n_levels * nsub), order_all((size_t)n_levels * nsub);
   const double *nu = ctx->nu.data();
-  for (int l = 0; l < n_levels; ++l)
+  for (int c = 0; c < n_chunks; ++c) {
+    const double Pmax = *std::max_element(P + lb[c], P + lb[c + 1]);
     for (int isub = 0; isub < nsub; ++isub) {
-      const double lo = pl.s[isub] - 1.0 - std::max(ctx->dmax, 0.0) * P[l] - 1e-6;
-      const double hi = pl.s[isub] + DELTA_WV + 1.0 - std::min(ctx->dmin, 0.0) * P[l] + 1e-6;
+      const double lo = pl.s[isub] - 1.0 - std::max(ctx->dmax, 0.0) * Pmax - 1e-6;
+      const double hi = pl.s[isub] + DELTA_WV + 1.0 - std::min(ctx->dmin, 0.0) * Pmax + 1e-6;
       int64_t a, b;
       ctx->nu_index.range(lo, N, a, b);
       const int64_t a0 = std::lower_bound(nu + a, nu + b, lo) - nu;
       ctx->nu_index.range(hi, N, a, b);
       const int64_t b0 = std::upper_bound(nu + std::max(a, a0), nu + std::max(b, a0), hi) - nu;
-      nbound[(size_t)l * nsub + isub] = (int)(b0 - a0);
+      for (int l = lb[c]; l < lb[c + 1]; ++l) nbound[(size_t)l * nsub + isub] = (int)(b0 - a0);
     }
+  }
   std::vector<int> tmp;
   for (int c = 0; c < n_chunks; ++c) {
     const int base = lb[c] * nsub, units = (lb[c + 1] - lb[c]) * nsub;
@@ -984,11 +999,13 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   CK(cudaStreamSynchronize(st), "stream sync");
   if (host_records) {
     CK(cudaStreamSynchronize(ctx->copy_stream), "copy stream sync");
-    // kernel and copy time per level, for the chunks of the next call
+    // kernel and copy time per level, for the chunks of the next call (the
+    // kernels' time from the call's first to its last kernel: the chunks'
+    // kernels overlap on two streams)
     double kms = 0.0, cms = 0.0;
     float ms = 0.f;
     for (auto &m : ctx->marks)
-      if (m.first <= 4 && cudaEventElapsedTime(&ms, m.second.first, m.second.second) == cudaSuccess) kms += ms;
+      if (m.first == 5 && cudaEventElapsedTime(&ms, m.second.first, m.second.second) == cudaSuccess) kms += ms;
     for (auto &m : copy_marks)
       if (cudaEventElapsedTime(&ms, m.first, m.second) == cudaSuccess) cms += ms;
     if (kms > 0.0 && cms > 0.0 && copy_marks.size() == (size_t)n_chunks) {
@@ -1152,8 +1169,10 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
     if (ctx->rec_ready[h]) cudaEventDestroy(ctx->rec_ready[h]);
     if (ctx->rec_copied[h]) cudaEventDestroy(ctx->rec_copied[h]);
   }
-  if (ctx->pinned) cudaFreeHost(ctx->pinned);
-  if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
+  for (int i = 0; i < marfa_ctx::NPIN; ++i) {
+    if (ctx->pinned[i]) cudaFreeHost(ctx->pinned[i]);
+    if (ctx->pinned_ev[i]) cudaEventDestroy(ctx->pinned_ev[i]);
+  }
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
