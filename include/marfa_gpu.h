@@ -170,8 +170,8 @@ void marfa_graph_destroy(marfa_graph *graph);
 
 /* Chooses the context's launch parameters that do not change the method --
  * lines per far-kernel block (far_chunk: 2048, 4096 or 8192) and the number of
- * coarse fine grids whose accumulators are summed by a whole warp (coop_k:
- * 1..5) -- by timing every candidate on up to four levels of the given
+ * coarse fine grids whose accumulators are summed by groups of lanes rather
+ * than one thread each (coop_k: 1..5) -- by timing every candidate on up to four levels of the given
  * profile, keeps the fastest in the context and returns it.  Results change
  * only by summation order (far-line sums are split differently).  No
  * reference counterpart (the reference has no launch parameters). */

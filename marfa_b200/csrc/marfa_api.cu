@@ -33,8 +33,7 @@ struct DevBuf {
 // Launch parameters that do not change results (chosen by marfa_autotune).
 struct Tune {
   int far_chunk = 4096;    // lines per far-kernel block
-  int coop_k = 3;          // fine grids whose sites are summed by one warp each
-  int group8_k = 4;        // the next fine grids up to this one: eight lanes per site
+  int coop_k = 5;          // fine grids whose sites are summed by lane groups
   int sparse_lines = 1024; // units with fewer near lines skip untouched sites
   int small_block_lines = 512; // batches whose units all have fewer near lines use small blocks
 };
@@ -865,7 +864,6 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.vbuf = B.vbuf->p;
     fn.queue = (int *)B.queue->p;
     fn.coop_k = ctx->tune.coop_k;
-    fn.group8_k = ctx->tune.group8_k;
     fn.sparse_lines = ctx->tune.sparse_lines;
     const int UBc = UB;
     for (int u0 = 0; u0 < units; u0 += UBc) {

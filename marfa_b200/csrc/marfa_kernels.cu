@@ -1132,10 +1132,16 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     const long long t1 = pc ? clock64() : 0;
     if (k <= 9) {
       const int ntk = nt_k(k), nsite = ntk + 1, cb = base_k(k) - NT0;
-      // lanes per cell: a warp on the coarsest grids, groups of 8 on the
-      // next ones, one thread on the dense grids and in sparse units (few
-      // lines per site)
-      const int G = sparse ? 1 : (k <= p.coop_k ? 32 : (k <= p.group8_k ? 8 : 1));
+      // lanes per cell on grids 1..coop_k: the largest power of two (at most
+      // a warp) with which all cells are summed in one round (about the same
+      // number of lines per lane on every grid: the lines per cell halve as
+      // the cells double); one thread per cell on the other grids and in
+      // sparse units (few lines per site)
+      int G = 1;
+      if (!sparse && k <= p.coop_k) {
+        const int want = (int)blockDim.x / nsite;
+        G = want >= 32 ? 32 : want >= 16 ? 16 : want >= 8 ? 8 : want >= 4 ? 4 : want >= 2 ? 2 : 1;
+      }
       if (G == 1) {
         for (int e = threadIdx.x; e < nsite; e += blockDim.x) {
           if (sparse && !is_touched(s_touched, e)) { // no contribution: zero accumulators
@@ -1152,8 +1158,14 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
         const int lane = threadIdx.x & (G - 1), grp = threadIdx.x / G, ngrp = blockDim.x / G;
         const int rounds = (nsite + ngrp - 1) / ngrp; // the same for every lane
         for (int r = 0; r < rounds; ++r) {
-          if (G == 32) gather_cell<F64, 32>(st, k, grp + r * ngrp, vb, vcap, scr, lane);
-          else gather_cell<F64, 8>(st, k, grp + r * ngrp, vb, vcap, scr, lane);
+          const int e = grp + r * ngrp;
+          switch (G) {
+          case 32: gather_cell<F64, 32>(st, k, e, vb, vcap, scr, lane); break;
+          case 16: gather_cell<F64, 16>(st, k, e, vb, vcap, scr, lane); break;
+          case 8: gather_cell<F64, 8>(st, k, e, vb, vcap, scr, lane); break;
+          case 4: gather_cell<F64, 4>(st, k, e, vb, vcap, scr, lane); break;
+          default: gather_cell<F64, 2>(st, k, e, vb, vcap, scr, lane); break;
+          }
         }
       }
     } else {

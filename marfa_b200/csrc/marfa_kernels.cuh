@@ -103,8 +103,7 @@ struct FineParams {
   int grid;                      // persistent blocks
   int vsm_rows;                  // slot-buffer rows held in shared memory (0, 10 or NSLOT)
   int sparse_lines;              // units with fewer staged lines skip untouched sites
-  int coop_k;                    // grids 1..coop_k: one warp per site in the site half
-  int group8_k;                  // grids coop_k+1..group8_k: eight lanes per site
+  int coop_k;                    // grids 1..coop_k: lane groups per site in the site half
   int block_threads;             // threads per block (fine_block_threads)
 };
 

@@ -361,8 +361,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   fn.order = nullptr;
   fn.grid = 1;
   fn.vsm_rows = 0;
-  fn.coop_k = 3;
-  fn.group8_k = 4;
+  fn.coop_k = 5;
   fn.sparse_lines = 1024;
   fn.block_threads = fine_block_threads(run->precision, 1 << 30, 0);
   fn.vbuf = base + OFF_VB;

@@ -65,24 +65,40 @@ def test_graph_refuses_a_changed_launch_plan(gpu):
 
 
 def test_autotune_keeps_results(gpu):
-    torch = pytest.importorskip("torch")
+    """The tuned launch parameters change only the order of summation: FP64
+    records stay within 1e-12 of the untuned ones, FP32c records within the
+    FP32c contract of the FP64 oracle (1e-5 away from near-tie clamps) with
+    and without tuning."""
+    import oracle as O
+    from fp32c_check import check_fp32c
+    from marfa_b200.io import species_code
     tips = read_tips(data_path("TIPS_subset.dat"))
     w = synth.config(1, 0.03)
     p = w.profiles[0]
     lv = [0, 13, 26, 39]
     P, T, n = (np.asarray(a, dtype=np.float64)[lv] for a in (p.pressure, p.temperature, p.density))
-    for prec, tol in (("fp32c", 1e-5), ("fp64", 1e-12)):
+    orc = O.Oracle(w.lines, tips, P, T, n, w.start_wv, w.end_wv, w.cutoff, target=w.target, chi=w.chi,
+                   mol_code=species_code(w.molecule), precision=O.FP64)
+    ref = orc.run()[1]
+    for prec in ("fp32c", "fp64"):
         run = Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule, chi=w.chi,
                   precision=prec)
         with Context(w.lines, tips) as ctx:
-            before = ctx.compute(run, P, T, n, want64=True)[1]
+            before = ctx.compute(run, P, T, n, want64=True)
             choice = ctx.autotune(run, P, T, n)
             assert choice["far_chunk"] in (2048, 4096, 8192)
             assert 1 <= choice["coop_k"] <= 5
-            after = ctx.compute(run, P, T, n, want64=True)[1]
-        big = before > 1e-6 * before.max()
-        rel = np.abs(after[big] - before[big]) / before[big]
-        assert rel.max() <= tol, (prec, choice, rel.max())
+            after = ctx.compute(run, P, T, n, want64=True)
+        if prec == "fp64":
+            b, a = before[1], after[1]
+            big = b > 1e-6 * b.max()
+            rel = np.abs(a[big] - b[big]) / b[big]
+            assert rel.max() <= 1e-12, (choice, rel.max())
+        else:
+            for got in (before[0], after[0]):
+                err, n_tainted = check_fp32c(got, ref, orc)
+                assert err <= 1e-5, (choice, err)
+                assert n_tainted <= 1e-4 * ref.size
 
 
 def test_host_record_chunks_keep_results(gpu):
