@@ -212,6 +212,117 @@ struct ChiPieces {
   }
 };
 
+// Pairs of floats in one 64-bit register for the packed FP32 instructions
+// of sm_100 (add/mul/fma .rn.f32x2: two lanes per instruction, each lane
+// rounded as the scalar instruction rounds it).
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 x2_pack(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void x2_unpack(f32x2 v, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 x2_add(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 x2_mul(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 x2_fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// Grid-0 sums of the far kernel's FP32 form: positions 2j and 2j + 1 in the
+// two lanes of acc[j] (j = 0 .. 9), position 20 in a20.
+struct FarAcc {
+  f32x2 acc[10];
+  float a20;
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int j = 0; j < 10; ++j) acc[j] = 0ull;
+    a20 = 0.f;
+  }
+  // v[k] at distance index k of a line left (position k) or right (position 20 - k)
+  __device__ __forceinline__ void add(const float (&v)[NFAR], bool left) {
+#pragma unroll
+    for (int j = 0; j < 10; ++j)
+      acc[j] = x2_add(acc[j], left ? x2_pack(v[2 * j], v[2 * j + 1]) : x2_pack(v[20 - 2 * j], v[19 - 2 * j]));
+    a20 += left ? v[20] : v[0];
+  }
+  // Lorentz (times chi = c 2^(r d), one piece) of one line at the 21
+  // distances d_k = fl((N 2^-11 + k/2) + f), two distances per instruction:
+  // left lines pair k = 2j, 2j + 1 (positions 2j, 2j + 1), right lines pair
+  // k = 19 - 2j, 20 - 2j (positions 2j + 1, 2j, stored swapped so that the
+  // lanes match).  ce carries cA 2^(r d_k) from pair to pair by 2^(r)
+  // (two distance steps of 1/2).
+  template <bool WITH_CHI>
+  __device__ __forceinline__ void lorentz(bool left, float Nf, float ff, float cA, float g2, float r) {
+    const f32x2 ff2 = x2_pack(ff, ff), g22 = x2_pack(g2, g2);
+    float e0 = 1.f, step = 1.f;
+    if (WITH_CHI) {
+      step = ex2_approx(0.5f * r);
+      e0 = ex2_approx(r * __fadd_rn(Nf, ff));
+    }
+    const float c0 = cA * e0, c1 = c0 * step;
+    const f32x2 step2 = x2_pack(step * step, step * step);
+    if (left) {
+      f32x2 base = x2_pack(Nf, Nf + 0.5f), ce = x2_pack(c0, c1);
+      const f32x2 one = x2_pack(1.f, 1.f);
+#pragma unroll
+      for (int j = 0; j < 10; ++j) {
+        const f32x2 d = x2_add(base, ff2);
+        const f32x2 den = x2_fma(d, d, g22);
+        float d0, d1;
+        x2_unpack(den, d0, d1);
+        acc[j] = x2_fma(ce, x2_pack(rcp_approx(d0), rcp_approx(d1)), acc[j]);
+        base = x2_add(base, one);
+        if (WITH_CHI) ce = x2_mul(ce, step2);
+      }
+      float cl, ch;
+      x2_unpack(ce, cl, ch);
+      const float d = __fadd_rn(Nf + 10.f, ff);
+      a20 += cl * rcp_approx(fmaf(d, d, g2));
+    } else {
+      // k = 0 at position 20, then pairs (k = 2j + 2, 2j + 1) at positions
+      // (18 - 2j, 19 - 2j) = acc[9 - j]
+      {
+        const float d = __fadd_rn(Nf, ff);
+        a20 += c0 * rcp_approx(fmaf(d, d, g2));
+      }
+      f32x2 base = x2_pack(Nf + 1.f, Nf + 0.5f), ce = x2_pack(c1 * step, c1);
+      const f32x2 one = x2_pack(1.f, 1.f);
+#pragma unroll
+      for (int j = 0; j < 10; ++j) {
+        const f32x2 d = x2_add(base, ff2);
+        const f32x2 den = x2_fma(d, d, g22);
+        float d0, d1;
+        x2_unpack(den, d0, d1);
+        acc[9 - j] = x2_fma(ce, x2_pack(rcp_approx(d0), rcp_approx(d1)), acc[9 - j]);
+        base = x2_add(base, one);
+        if (WITH_CHI) ce = x2_mul(ce, step2);
+      }
+    }
+  }
+  __device__ __forceinline__ void store(double (&res)[NFAR]) const {
+#pragma unroll
+    for (int j = 0; j < 10; ++j) {
+      float lo, hi;
+      x2_unpack(acc[j], lo, hi);
+      res[2 * j] = (double)lo;
+      res[2 * j + 1] = (double)hi;
+    }
+    res[20] = (double)a20;
+  }
+};
+
 template <bool F64, int CHI>
 __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
   const int item = blockIdx.x;
@@ -267,9 +378,8 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
   } else {
     // plain float sums: one thread adds FAR_CHUNK / 256 lines per position
     // (16 at the default chunk), the block reduction then runs in double
-    float acc[NFAR];
-#pragma unroll
-    for (int k = 0; k < NFAR; ++k) acc[k] = 0.f;
+    FarAcc fa;
+    fa.init();
     const ChiPieces<CHI> pc(lv);
     for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
       double D;
@@ -283,19 +393,7 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
         const float Nf = (float)(Nd * (1.0 / 2048.0));
         const float ff = (float)(D - Nd * (1.0 / 2048.0));
         if (CHI == CHI_NONE) {
-          float F[NFAR];
-#pragma unroll
-          for (int k = 0; k < NFAR; ++k) {
-            const float d = __fadd_rn(Nf + 0.5f * k, ff);
-            F[k] = h.lorA * rcp_approx(fmaf(d, d, h.g2));
-          }
-          if (left) {
-#pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[k] += F[k];
-          } else {
-#pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k] += F[k];
-          }
+          fa.lorentz<false>(left, Nf, ff, h.lorA, h.g2, 0.f);
         } else {
           int kb[3];
 #pragma unroll
@@ -306,21 +404,14 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
             kb[j] = j >= pc.nb || D + 10.0 < bj - 1e-6 ? NFAR
                   : (D > bj + 1e-6 ? 0 : first_k_past(D, bj, pc.strict[j]));
           }
-          float F[NFAR];
-          if (kb[0] == 0 && kb[1] == NFAR) { // one chi piece over the whole line
-            // chi(d + k/2) = chi(d) * 2^(r/2)^k: one exponential per line, the
-            // factor of each next position by one multiplication (relative
-            // error below 1e-6 after the 20 steps)
-            const float cA = h.lorA * pc.c[1], r = pc.r[1];
-            const float step = ex2_approx(0.5f * r);
-            float e = ex2_approx(r * __fadd_rn(Nf, ff));
-#pragma unroll
-            for (int k = 0; k < NFAR; ++k) {
-              const float d = __fadd_rn(Nf + 0.5f * k, ff);
-              F[k] = (cA * rcp_approx(fmaf(d, d, h.g2))) * e;
-              e *= step;
-            }
+          if (kb[0] == 0 && kb[1] == NFAR) {
+            // one chi piece over the whole line: chi(d + k/2) = chi(d) *
+            // 2^(r/2)^k, one exponential per line and the factor of each
+            // next pair of positions by one multiplication (relative error
+            // below 1e-6 after the ten steps)
+            fa.lorentz<true>(left, Nf, ff, h.lorA * pc.c[1], h.g2, pc.r[1]);
           } else {
+            float F[NFAR];
 #pragma unroll
             for (int k = 0; k < NFAR; ++k) {
               const float d = __fadd_rn(Nf + 0.5f * k, ff);
@@ -329,13 +420,7 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
               const float rr = pcs == 0 ? pc.r[0] : (pcs == 1 ? pc.r[1] : (pcs == 2 ? pc.r[2] : pc.r[3]));
               F[k] = (h.lorA * cc * rcp_approx(fmaf(d, d, h.g2))) * ex2_approx(rr * d);
             }
-          }
-          if (left) {
-#pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[k] += F[k];
-          } else {
-#pragma unroll
-            for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k] += F[k];
+            fa.add(F, left);
           }
         }
       } else {
@@ -348,17 +433,10 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
           else if (p.shape == 101) F[k] = (float)d;
           else F[k] = voigt_general<float, CHI>(d, g, lv, p.c, p.sscale);
         }
-        if (left) {
-#pragma unroll
-          for (int k = 0; k < NFAR; ++k) acc[k] += F[k];
-        } else {
-#pragma unroll
-          for (int k = 0; k < NFAR; ++k) acc[NFAR - 1 - k] += F[k];
-        }
+        fa.add(F, left);
       }
     }
-#pragma unroll
-    for (int k = 0; k < NFAR; ++k) res[k] = (double)acc[k];
+    fa.store(res);
   }
   block_reduce_store<NFAR>(res, p.out + ((size_t)l * p.n_chunks + ci) * NFAR);
 }
