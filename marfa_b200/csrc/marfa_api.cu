@@ -519,8 +519,8 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     Lc = o.graph->Lc;
     UB = o.graph->UB;
   }
-  // host records: at least four chunks of levels, so that the copy of each
-  // overlaps the computation of the next
+  // host records: chunks of levels (level_chunk_sizes), so that the copy of
+  // each overlaps the computation of the next
   const bool host_records = o.host_out != nullptr && !adj;
   const bool two = host_records && !o.host_out64 && !o.host_dump && !o.graph && n_levels >= 2;
   if (two) { // two buffer sets in the same memory
@@ -537,8 +537,9 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   for (int c : csz) lb.push_back(lb.back() + c);
   const int n_chunks = (int)csz.size();
   if (host_records) {
-    Lc = *std::max_element(csz.begin(), csz.end()); // largest chunk: sizes the record halves
-    UB = std::min(UB, Lc * nsub);
+    // buffers keep the planned chunk size Lc (no chunk exceeds it), so that a
+    // changed schedule on a later call reallocates nothing
+    UB = std::min(UB, *std::max_element(csz.begin(), csz.end()) * nsub);
     if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
     for (int h = 0; h < 2; ++h) {
       if (!ctx->rec_ready[h]) CK(cudaEventCreateWithFlags(&ctx->rec_ready[h], cudaEventDisableTiming), "event");
