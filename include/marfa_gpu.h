@@ -138,7 +138,10 @@ int marfa_compute_batched(marfa_ctx *ctx, const marfa_run *run, int n_profiles,
 
 /* Same as marfa_compute_batched with a DEVICE output buffer, enqueued on
  * `stream` (a cudaStream_t; NULL = the context's stream) and returning
- * without waiting; the inputs are host arrays copied inside the call. */
+ * without waiting; the inputs are host arrays copied inside the call (through
+ * a ring of four pinned buffers: up to four calls queue ahead of the device
+ * before a call waits).  Consecutive calls on one context use one stream: the
+ * per-call tables live in the context. */
 int marfa_compute_device(marfa_ctx *ctx, const marfa_run *run, int n_profiles,
                          const int *level_counts, const double *pressure,
                          const double *temperature, const double *density,
