@@ -122,3 +122,33 @@ def test_host_record_chunks_keep_results(gpu):
             ctx.compute(run, P, T, n, out=host)
             assert torch.equal(host, ref)
         assert float(ref.abs().sum()) > 0.0
+
+
+def test_queued_device_calls(gpu):
+    """Device calls queue on the stream without waiting (a ring of pinned
+    staging buffers carries their tables): six calls with different profiles
+    enqueued back to back give the records of the same calls made one at a
+    time."""
+    torch = pytest.importorskip("torch")
+    tips = read_tips(data_path("TIPS_subset.dat"))
+    w = synth.config(1, 0.03)
+    p = w.profiles[0]
+    P, T, n = (np.asarray(a, dtype=np.float64) for a in (p.pressure, p.temperature, p.density))
+    run = Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule, chi=w.chi,
+              precision="fp32c")
+    shape = (len(P), run.n_sub, 20481)
+    pressures = [P * (1.0 + 0.05 * i) for i in range(6)]
+    with Context(w.lines, tips) as ctx:
+        one = []
+        for Pi in pressures:
+            o = torch.empty(shape, dtype=torch.float32, device="cuda")
+            ctx.compute_device(run, [len(P)], Pi, T, n, o.data_ptr())
+            ctx.synchronize()
+            one.append(o)
+        queued = [torch.empty(shape, dtype=torch.float32, device="cuda") for _ in pressures]
+        for Pi, o in zip(pressures, queued):
+            ctx.compute_device(run, [len(P)], Pi, T, n, o.data_ptr())
+        ctx.synchronize()
+        for a, b in zip(one, queued):
+            assert torch.equal(a, b)
+        assert not torch.equal(one[0], one[5])
