@@ -172,7 +172,7 @@ int marfa_graph_launch(marfa_graph *graph, const double *pressure, const double 
 void marfa_graph_destroy(marfa_graph *graph);
 
 /* Chooses the context's launch parameters that do not change the method --
- * lines per far-kernel block (far_chunk: 2048, 4096 or 8192) and the number of
+ * lines per far-kernel block (far_chunk: 2048, 4096, 8192 or 16384) and the number of
  * coarse fine grids whose accumulators are summed by groups of lanes rather
  * than one thread each (coop_k: 1..5) -- by timing every candidate on up to four levels of the given
  * profile, keeps the fastest in the context and returns it.  Results change

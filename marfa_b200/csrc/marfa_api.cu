@@ -32,7 +32,7 @@ struct DevBuf {
 
 // Launch parameters that do not change results (chosen by marfa_autotune).
 struct Tune {
-  int far_chunk = 4096;    // lines per far-kernel block
+  int far_chunk = 16384;   // lines per far-kernel block
   int coop_k = 5;          // fine grids whose sites are summed by lane groups
   int sparse_lines = 1024; // units with fewer near lines skip untouched sites
   int small_block_lines = 512; // batches whose units all have fewer near lines use small blocks
@@ -1399,7 +1399,7 @@ int marfa_autotune(marfa_ctx *ctx, const marfa_run *run, int n_levels, const dou
   const Tune keep = ctx->tune;
   Tune best = keep;
   double best_ms = 1e300;
-  for (int fcv : {2048, 4096, 8192})
+  for (int fcv : {2048, 4096, 8192, 16384})
     for (int ck : {1, 2, 3, 4, 5}) {
       ctx->tune.far_chunk = fcv;
       ctx->tune.coop_k = ck;

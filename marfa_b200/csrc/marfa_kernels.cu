@@ -376,8 +376,9 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
 #pragma unroll
     for (int k = 0; k < NFAR; ++k) res[k] = acc[k];
   } else {
-    // plain float sums: one thread adds FAR_CHUNK / 256 lines per position
-    // (16 at the default chunk), the block reduction then runs in double
+    // plain float sums: one thread adds (lines per block) / 256 lines per
+    // position (64 at the default 16,384), the block reduction then runs in
+    // double
     FarAcc fa;
     fa.init();
     const ChiPieces<CHI> pc(lv);

@@ -86,7 +86,7 @@ def test_autotune_keeps_results(gpu):
         with Context(w.lines, tips) as ctx:
             before = ctx.compute(run, P, T, n, want64=True)
             choice = ctx.autotune(run, P, T, n)
-            assert choice["far_chunk"] in (2048, 4096, 8192)
+            assert choice["far_chunk"] in (2048, 4096, 8192, 16384)
             assert 1 <= choice["coop_k"] <= 5
             after = ctx.compute(run, P, T, n, want64=True)
         if prec == "fp64":
