@@ -559,7 +559,10 @@ __global__ void __launch_bounds__(256) near_adjoint_kernel(AdjointParams p) {
   const double *gs = p.gscratch + (size_t)ub * SCR_STRIDE;
   const LevelConst lv = p.lv[l];
   __shared__ int64_t sb[4];
-  if (threadIdx.x < 4) sb[threadIdx.x] = near_bound(snu, p.n_lines, s, se, threadIdx.x);
+  if (threadIdx.x < 128) { // warp w finds bound w
+    const int64_t v = near_bound_warp(snu, p.n_lines, s, se, threadIdx.x >> 5);
+    if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = v;
+  }
   __syncthreads();
   const int64_t a = sb[0], b = sb[3];
   double tT = 0.0, tP = 0.0;

@@ -353,6 +353,38 @@ __device__ __forceinline__ int64_t near_bound(const double *snu, int64_t n, doub
   return lo;
 }
 
+// near_bound by one warp: each step probes 32 evenly spaced positions of
+// the remaining range at once (the predicate is monotone: false ... true),
+// so that about four dependent loads replace a binary search's eighteen.
+// Every lane of the warp calls it and gets the result.
+__device__ __forceinline__ int64_t near_bound_warp(const double *snu, int64_t n, double s, double se, int which) {
+  const int lane = threadIdx.x & 31;
+  auto pred = [&](double v) {
+    if (which == 0) return !(v < s && (v - s) <= -1.0);
+    if (which == 1) return v >= s;
+    if (which == 2) return v > se;
+    return v > se && ((v - s) - DELTA_WV) >= 1.0;
+  };
+  int64_t lo = 0, hi = n; // the answer lies in [lo, hi]
+  while (hi - lo > 32) {
+    const int64_t span = hi - lo;
+    const int64_t pos = lo + (span * (lane + 1)) / 33; // in [lo, hi)
+    const unsigned b = __ballot_sync(0xffffffffu, pred(snu[pos]));
+    if (b) {
+      const int f = __ffs(b) - 1;
+      const int64_t pf = lo + (span * (f + 1)) / 33;
+      const int64_t pp = f > 0 ? lo + (span * f) / 33 + 1 : lo;
+      lo = pp;
+      hi = pf;
+    } else {
+      lo = lo + (span * 32) / 33 + 1;
+    }
+  }
+  const int64_t pos = lo + lane;
+  const unsigned b = __ballot_sync(0xffffffffu, pos < hi && pred(snu[pos]));
+  return b ? lo + (__ffs(b) - 1) : hi;
+}
+
 // Whether near line `li` (shifted centre v) contributes to the subinterval:
 // inside the line window, within the cutoff (left side keeps D == cutoff,
 // right side drops it: LineGridCalc.f90:23, 509), centre lines with UU < 10.

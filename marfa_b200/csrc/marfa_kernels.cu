@@ -1083,7 +1083,10 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   __shared__ int64_t sb[4];
   __shared__ int s_counts[2];
   // [a, c0): near-left; [c0, c1): centre; [c1, b): near-right (sorted order)
-  if (threadIdx.x < 4) sb[threadIdx.x] = near_bound(snu, p.n_lines, s, se, threadIdx.x);
+  if (threadIdx.x < 128) { // warp w finds bound w
+    const int64_t v = near_bound_warp(snu, p.n_lines, s, se, threadIdx.x >> 5);
+    if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = v;
+  }
   if (threadIdx.x < 2) s_counts[threadIdx.x] = 0;
   __syncthreads();
   const int64_t a = sb[0], b = sb[3];
