@@ -338,25 +338,10 @@ __device__ __forceinline__ double walk_hi(int j, double hk) { return (double)(2 
 // order: which = 0 first line with nu' > s - 1 (or inside), 1 first with
 // nu' >= s, 2 first with nu' > se, 3 first line at least 1 cm-1 right of the
 // subinterval.  [b0, b1) near-left, [b1, b2) centre, [b2, b3) near-right.
-__device__ __forceinline__ int64_t near_bound(const double *snu, int64_t n, double s, double se, int which) {
-  int64_t lo = 0, hi = n;
-  while (lo < hi) {
-    const int64_t m = (lo + hi) >> 1;
-    const double v = snu[m];
-    bool pr;
-    if (which == 0) pr = !(v < s && (v - s) <= -1.0);
-    else if (which == 1) pr = v >= s;
-    else if (which == 2) pr = v > se;
-    else pr = v > se && ((v - s) - DELTA_WV) >= 1.0;
-    if (pr) hi = m; else lo = m + 1;
-  }
-  return lo;
-}
-
-// near_bound by one warp: each step probes 32 evenly spaced positions of
-// the remaining range at once (the predicate is monotone: false ... true),
-// so that about four dependent loads replace a binary search's eighteen.
-// Every lane of the warp calls it and gets the result.
+// Found by one warp: each step probes 32 evenly spaced positions of the
+// remaining range at once (the predicate is monotone: false ... true), so
+// that about four dependent loads replace a binary search's eighteen.  Every
+// lane of the warp calls it and gets the result.
 __device__ __forceinline__ int64_t near_bound_warp(const double *snu, int64_t n, double s, double se, int which) {
   const int lane = threadIdx.x & 31;
   auto pred = [&](double v) {
