@@ -1081,13 +1081,11 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   const double s = p.win.sub_s[sub], se = p.win.sub_e[sub], cut = p.cutoff;
   const int64_t wlo = p.win.lo[sub], whi = p.win.hi[sub];
   __shared__ int64_t sb[4];
-  __shared__ int s_counts[2];
   // [a, c0): near-left; [c0, c1): centre; [c1, b): near-right (sorted order)
   if (threadIdx.x < 128) { // warp w finds bound w
     const int64_t v = near_bound_warp(snu, p.n_lines, s, se, threadIdx.x >> 5);
     if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = v;
   }
-  if (threadIdx.x < 2) s_counts[threadIdx.x] = 0;
   __syncthreads();
   const int64_t a = sb[0], b = sb[3];
   const int cnt = (int)(b - a);
@@ -1111,25 +1109,28 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   st.sqrt14 = p.c.sqrt14;
   const double sscale = F64 ? 1.0 : p.sscale;
   // compaction: lines inside the window, within the cutoff, able to contribute
-  int m_total = 0;
+  int m_total = 0, c0 = 0, c1 = 0;
   for (int64_t q0 = a; q0 < b; q0 += blockDim.x) {
     const int64_t q = q0 + threadIdx.x;
     int keep = 0, cls = 1;
     double UU = 0.0;
     int64_t li = 0;
+    LineGen g{};
     if (q < b) {
       li = sidx[q];
       keep = near_keep(snu[q], li, s, se, cut, wlo, whi, UU, cls);
+      if (keep && p.shape == 0) g = gen[li]; // in flight during the scan
     }
     int tot;
     const int pos = m_total + block_excl_scan(keep, tot);
-    if (keep && pos < cap) {
+    const bool put = keep && pos < cap;
+    if (put) {
       st.uu[pos] = UU;
       // bins of the centre lines (UU in [0, 10)): at most 20480
       n11[pos] = cls == 1 ? (short)(int)floor(UU * 2048.0) : (short)0;
       nv11[pos] = cls == 1 ? (short)(int)floor((DELTA_WV - UU) * 2048.0) : (short)0;
       if (p.shape == 0) {
-        const ShapeP<Real> sp = shape_params<Real>(gen[li], p.c, sscale);
+        const ShapeP<Real> sp = shape_params<Real>(g, p.c, sscale);
         st.qx[pos] = sp.qx;
         st.vy[pos] = sp.vy;
         st.lorA[pos] = sp.lorA;
@@ -1140,15 +1141,15 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
         st.vy[pos] = p.shape == 100 ? -1.0 : 1.0;
         st.lorA[pos] = st.g2[pos] = st.hum[pos] = (Real)0;
       }
-      if (cls == 0) atomicAdd(&s_counts[0], 1);
-      if (cls != 2) atomicAdd(&s_counts[1], 1);
     }
+    // staged lines of each class (block-wide counts, one barrier each)
+    c0 += __syncthreads_count(put && cls == 0);
+    c1 += __syncthreads_count(put && cls != 2);
     m_total += tot;
   }
-  __syncthreads();
   st.m = min(m_total, cap);
-  st.c0 = s_counts[0];
-  st.c1 = s_counts[1];
+  st.c0 = c0;
+  st.c1 = c1;
   Real *scr = (Real *)p.scratch + (size_t)ub * SCR_STRIDE;
   if (m_total > cap) { // cannot happen when the host sized the staging area
     if (threadIdx.x == 0) atomicMax(p.err, 14);
