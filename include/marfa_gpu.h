@@ -62,8 +62,8 @@ extern "C" {
 
 /* arithmetic of the line-shape accumulation */
 #define MARFA_PREC_FP64 0   /* every quantity in double: the drop-in          */
-#define MARFA_PREC_FP32C 1  /* FP32 shapes, Kahan FP32 sums; FP64 prep,       */
-                            /* offsets and cascade                            */
+#define MARFA_PREC_FP32C 1  /* FP32 shapes and FP32 partial sums reduced in   */
+                            /* double; FP64 prep, offsets and cascade         */
 
 #define MARFA_NT 20481      /* points per PT record (Grids.f90:16)            */
 

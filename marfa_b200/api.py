@@ -29,7 +29,7 @@ class Run:
     molecule: str = "CO2"
     chi: str = "none"
     shape: str = "voigt"
-    precision: str = "fp32c"
+    precision: str = "fp64"
 
     def c(self) -> MarfaRun:
         code = species_code(self.molecule)

@@ -646,11 +646,15 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     if (fc.max_near > 65535) // line indices of one unit are 16-bit in the fine kernel's bin table
       return set_err(ctx, MARFA_E_CAPACITY, "%d lines within 1 cm-1 of one subinterval (at most 65535)",
                      fc.max_near);
-    const int smem_max = f64 ? 4096 : 2688;
-    fc.smem_cap = std::max(256, std::min(smem_max, (fc.max_near + 127) / 128 * 128));
+    fc.block_threads = fine_block_threads(run->precision, fc.max_near, ctx->tune.small_block_lines);
+    // on-chip staging up to 4096 (FP64) / 2688 (FP32c) lines, and never past
+    // what the block's shared memory holds beside the kernel's static arrays
+    int smem_lines = 0;
+    CK(fine_smem_lines(run->precision, chi, fc.block_threads, &smem_lines), "fine shared memory");
+    const int smem_max = std::min(f64 ? 4096 : 2688, smem_lines);
+    fc.smem_cap = std::max(128, std::min(smem_max, (fc.max_near + 127) / 128 * 128));
     fc.gstage_cap = fc.max_near > fc.smem_cap ? (fc.max_near + 255) / 256 * 256 : 0;
     fc.gstage_bytes = fc.gstage_cap ? fine_smem_bytes(fc.gstage_cap, f64) : 0;
-    fc.block_threads = fine_block_threads(run->precision, fc.max_near, ctx->tune.small_block_lines);
     CK(fine_plan(run->precision, chi, fc.block_threads, fc.smem_cap, &fc.vsm_rows, &fc.resident), "fine occupancy");
     gstage_need = std::max(gstage_need, (size_t)fc.resident * fc.gstage_bytes);
     vbuf_need = std::max(vbuf_need, (size_t)fc.resident *

@@ -2,7 +2,7 @@
 // (app/main.f90) driving libmarfa_gpu.so through its C ABI.
 //
 //   marfa Molecule StartWV EndWV DatabaseSlug CutOff TargetValue AtmProfileFile
-//         [precision fp32c|fp64] [chi none|tonkov|pollack|perrin] [device]
+//         [precision fp64|fp32c] [chi none|tonkov|pollack|perrin] [device]
 //
 // Same positional arguments, input paths (data/databases/<slug>.<NN>,
 // data/Atmospheres/<file>, data/TIPS/TIPS.dat relative to the working
@@ -65,7 +65,7 @@ void usage(int argc) {
   std::printf(" Insufficient number of arguments.\n");
   std::printf(" Expected at least 7 arguments, but received %d\n", argc);
   std::printf(" Usage: marfa Molecule StartWV EndWV DatabaseSlug CutOff TargetValue AtmProfileFile\n");
-  std::printf("        [precision fp32c|fp64] [chi none|tonkov|pollack|perrin] [device]\n");
+  std::printf("        [precision fp64|fp32c] [chi none|tonkov|pollack|perrin] [device]\n");
 }
 
 } // namespace
@@ -80,7 +80,8 @@ int main(int argc, char **argv) {
   const std::string start_txt = trim(argv[2]), end_txt = trim(argv[3]);
   const std::string slug = trim(argv[4]), cut_txt = trim(argv[5]);
   const std::string target = trim(argv[6]), profile_file = trim(argv[7]);
-  const std::string precision = nargs >= 8 ? trim(argv[8]) : "fp32c";
+  // FP64 is the drop-in arithmetic; fp32c is the faster form, opted into
+  const std::string precision = nargs >= 8 ? trim(argv[8]) : "fp64";
   const std::string chi_name = nargs >= 9 ? trim(argv[9]) : "none";
   const int device = nargs >= 10 ? std::atoi(argv[10]) : 0;
   char *e1 = nullptr, *e2 = nullptr, *e3 = nullptr;

@@ -1669,6 +1669,27 @@ static cudaError_t fine_occupancy_th(int smem_cap, int *rows, int *blocks) {
   return cudaSuccess;
 }
 
+// Most near lines one block stages in shared memory: the opt-in limit per
+// block minus the kernel's static shared memory, over the bytes per line.
+template <bool F64, int CHI, int TH>
+static cudaError_t fine_stage_limit_th(int *lines) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI, TH>);
+  if (e != cudaSuccess) return e;
+  int dev = 0, optin = 0;
+  if ((e = cudaGetDevice(&dev))) return e;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+  const size_t room = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  *lines = (int)(room / fine_smem_bytes(1, F64, 0)) / 128 * 128;
+  return cudaSuccess;
+}
+
+template <bool F64, int CHI>
+static cudaError_t fine_stage_limit(int threads, int *lines) {
+  return threads == SMALL_TH ? fine_stage_limit_th<F64, CHI, SMALL_TH>(lines)
+                             : fine_stage_limit_th<F64, CHI, fine_threads(F64)>(lines);
+}
+
 template <bool F64, int CHI>
 static cudaError_t fine_occupancy(int threads, int smem_cap, int *rows, int *blocks) {
   return threads == SMALL_TH ? fine_occupancy_th<F64, CHI, SMALL_TH>(smem_cap, rows, blocks)
@@ -1703,6 +1724,16 @@ size_t fine_vbuf_elems(int cap) { return (size_t)NSLOT * cap; }
 
 int fine_block_threads(int precision, int max_near, int small_below) {
   return max_near < small_below ? SMALL_TH : fine_threads(precision == 0);
+}
+
+cudaError_t fine_smem_lines(int precision, int chi, int threads, int *lines) {
+  const bool f64 = precision == 0;
+  switch (chi) {
+  case CHI_TONKOV: return f64 ? fine_stage_limit<true, CHI_TONKOV>(threads, lines) : fine_stage_limit<false, CHI_TONKOV>(threads, lines);
+  case CHI_POLLACK: return f64 ? fine_stage_limit<true, CHI_POLLACK>(threads, lines) : fine_stage_limit<false, CHI_POLLACK>(threads, lines);
+  case CHI_PERRIN: return f64 ? fine_stage_limit<true, CHI_PERRIN>(threads, lines) : fine_stage_limit<false, CHI_PERRIN>(threads, lines);
+  default: return f64 ? fine_stage_limit<true, CHI_NONE>(threads, lines) : fine_stage_limit<false, CHI_NONE>(threads, lines);
+  }
 }
 
 cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, int *vsm_rows, int *blocks) {

@@ -207,6 +207,9 @@ size_t fine_vbuf_elems(int cap);
 // block size of the fine kernel for a batch whose units have at most
 // `max_near` near lines (small blocks below `small_below` lines)
 int fine_block_threads(int precision, int max_near, int small_below);
+// most near lines a block of `threads` stages in shared memory (the opt-in
+// limit minus the kernel's static shared memory)
+cudaError_t fine_smem_lines(int precision, int chi, int threads, int *lines);
 // slot-buffer rows that fit in shared memory and the persistent grid size
 cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, int *vsm_rows, int *blocks);
 cudaError_t fma_peak(bool f64, double *flops_per_s);

@@ -348,8 +348,11 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
         !ck(cudaStreamSynchronize(st), "sync near"))
       return rc;
   }
-  const int smem_max = f64 ? 4096 : 2816;
-  fn.smem_cap = std::max(256, std::min(smem_max, (near + 127) / 128 * 128));
+  fn.block_threads = fine_block_threads(run->precision, 1 << 30, 0);
+  int smem_lines = 0;
+  if (!ck(fine_smem_lines(run->precision, chi, fn.block_threads, &smem_lines), "fine shared memory")) return rc;
+  const int smem_max = std::min(f64 ? 4096 : 2816, smem_lines);
+  fn.smem_cap = std::max(128, std::min(smem_max, (near + 127) / 128 * 128));
   if (near > fn.smem_cap) {
     if (near > GSTAGE_LINES)
       return fail(msg, msg_len, MARFA_E_CAPACITY, "%d lines near the subinterval exceed the static capacity of %d",
@@ -363,7 +366,6 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   fn.vsm_rows = 0;
   fn.coop_k = 5;
   fn.sparse_lines = 1024;
-  fn.block_threads = fine_block_threads(run->precision, 1 << 30, 0);
   fn.vbuf = base + OFF_VB;
   fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
   fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);

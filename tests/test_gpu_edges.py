@@ -1,0 +1,155 @@
+"""GPU parity on the hardest inputs of the reference's schedule:
+
+* lines exactly on the multigrid decision boundaries and at exactly the
+  cutoff distance (LineGridCalc.f90:23 keeps D == cutOff on the left, :509
+  drops U == cutOff on the right), at cutoffs 25 and 0.75;
+* positive and negative pressure shifts large enough (|delta| P up to
+  0.92 cm-1 at 92 atm) to reorder lines and move them across subinterval
+  edges: the window exit uses the unshifted centre (LBL.f90:57), the
+  placement the shifted one (LBL.f90:81-98, Spectroscopy.f90:38-49);
+* a dense band of 5,000 lines within one subinterval and 1 cm-1 around it
+  (more near lines than the fine kernel stages on chip);
+* the full Venus workload (200,000 lines, 40 levels x 100 subintervals).
+
+Tolerances: FP64 1e-12 relative on every point against the all-double
+oracle; placement exact (F = 1 counts) and F = |X| sums to 1e-12; FP32c
+1e-5 relative where k > 1e-6 max(k), outside the cascade near-tie points
+that fp32c_check identifies from the oracle's own accumulators.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_err
+from edge_cases import END, START, tie_lines
+from fp32c_check import check_fp32c
+from marfa_b200 import synth
+from marfa_b200.api import Context, Run, plan_windows
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+FP32C_TOL = 1e-5
+
+
+def profile(P, T):
+    P = synth.f32(P)
+    T = synth.f32(T)
+    return synth.Profile(P, T, synth.ideal_gas_density(P, T))
+
+
+def check_all(ctx, lines, tips, prof, start, end, cutoff, chi="none", target="ACS",
+              placement_subs=(), placement_levels=(0,)):
+    """FP64 records, placement (F = 1, F = |X|) and FP32c against the
+    oracle for one profile."""
+    kw = dict(target=target, chi=chi)
+    orc = O.Oracle(lines, tips, prof.pressure, prof.temperature, prof.density, start, end,
+                   cutoff, precision=O.FP64, **kw)
+    _, ref, _ = orc.run()
+    run = dict(start_wv=start, end_wv=end, cutoff=cutoff, molecule="CO2", **kw)
+    _, g64 = ctx.compute(Run(precision="fp64", **run), prof.pressure, prof.temperature,
+                         prof.density, want64=True)
+    err, n = rel_err(g64, ref, 0.0)
+    assert n == ref.size
+    assert err <= FP64_TOL, err
+    for shape in ("one", "absx"):
+        o = O.Oracle(lines, tips, prof.pressure, prof.temperature, prof.density, start, end,
+                     cutoff, precision=O.FP64, shape=shape, **kw)
+        for lvl in placement_levels:
+            for isub in placement_subs:
+                want = o.accumulators(lvl, isub)
+                got = ctx.accumulators(Run(precision="fp64", shape=shape, **run), prof.pressure,
+                                       prof.temperature, prof.density, lvl, isub)
+                if shape == "one":
+                    bad = np.flatnonzero(got != want)
+                    assert bad.size == 0, (lvl, isub, bad[:20])
+                else:
+                    assert np.array_equal(got > 0, want > 0), (lvl, isub)
+                    m = want > 0
+                    assert np.max(np.abs(got[m] - want[m]) / want[m]) <= FP64_TOL
+    g32 = ctx.compute(Run(precision="fp32c", **run), prof.pressure, prof.temperature, prof.density)
+    e32, n_taint = check_fp32c(g32, ref, orc, tol=FP32C_TOL)
+    assert e32 <= FP32C_TOL, e32
+    assert n_taint <= 1e-4 * ref.size
+    return ref
+
+
+@pytest.mark.parametrize("cutoff", [25.0, 0.75])
+def test_tie_lines_match_oracle(gpu, tips, cutoff):
+    lines = tie_lines(cutoff)
+    # 1 atm (Lorentz-dominated cores) and 1e-3 atm at 200 K (Humlicek
+    # regions 3 and 4 at the tie offsets)
+    prof = profile([1.0, 1e-3], [296.0, 200.0])
+    with Context(lines, tips) as ctx:
+        check_all(ctx, lines, tips, prof, START, END, cutoff, placement_subs=(0, 1, 2),
+                  placement_levels=(0, 1))
+
+
+@pytest.mark.parametrize("delta", [0.01, -0.01])
+def test_tie_lines_with_large_shift(gpu, tips, delta):
+    """Every line shifted by delta * 92 atm = +-0.92 cm-1: tie lines of the
+    middle subinterval move across both of its edges."""
+    lines = tie_lines(25.0, delta=delta)
+    prof = profile([92.0, 30.0], [735.0, 690.0])
+    with Context(lines, tips) as ctx:
+        check_all(ctx, lines, tips, prof, START, END, 25.0, placement_subs=(0, 1, 2),
+                  placement_levels=(0, 1))
+
+
+def test_random_shifts_both_signs(gpu, tips):
+    """delta uniform in [-0.01, 0.01] cm-1/atm at 92, 20 and 1 atm: lines
+    reorder by their shifted centres, and the window (unshifted) differs
+    from the placement (shifted)."""
+    lines = synth.make_lines(synth.LineSpec(n=20_000, nu_lo=3850.0, nu_hi=4250.0,
+                                            delta=(-0.01, 0.01), seed=21))
+    nus = lines["nu"][:-1] + lines["delta"][:-1].astype(np.float64) * 92.0
+    assert np.any(np.diff(nus) < 0)                  # the shift reorders lines
+    lo, hi = plan_windows(lines["nu"], 4000.0, 4100.0, 125.0)
+    o = O.Oracle(lines, tips, [92.0], [735.0], [1e20], 4000.0, 4100.0, 125.0)
+    olo, ohi = o.windows()
+    assert np.array_equal(lo, olo - 1) and np.array_equal(hi, ohi - 1)
+    prof = profile([92.0, 20.0, 1.0], [735.0, 650.0, 400.0])
+    with Context(lines, tips) as ctx:
+        check_all(ctx, lines, tips, prof, 4000.0, 4100.0, 125.0, chi="tonkov", target="VAC",
+                  placement_subs=(0, 5, 9))
+
+
+def dense_band(n=5000, seed=31):
+    """n lines within [4049, 4061]: all of them near lines of the
+    subinterval [4050, 4060)."""
+    return synth.make_lines(synth.LineSpec(n=n, nu_lo=4049.0, nu_hi=4061.0, seed=seed))
+
+
+def test_dense_band_beyond_on_chip_staging(gpu, tips):
+    lines = dense_band()
+    prof = profile([1.0, 0.01], [296.0, 250.0])
+    with Context(lines, tips) as ctx:
+        check_all(ctx, lines, tips, prof, START, END, 25.0, placement_subs=(1,))
+
+
+def test_full_venus_workload(gpu, tips):
+    """All 40 levels x 100 subintervals of the Venus workload: FP64 against
+    the all-double oracle on every point, FP32c within 1e-5 outside the
+    cascade near-tie points (their count is printed)."""
+    w = synth.config(1)
+    p = w.profiles[0]
+    orc = O.from_workload(w, precision=O.FP64, tips=tips)
+    _, ref, ev = orc.run()
+    run = dict(start_wv=w.start_wv, end_wv=w.end_wv, cutoff=w.cutoff, target=w.target,
+               molecule=w.molecule, chi=w.chi)
+    with Context(w.lines, tips) as ctx:
+        assert ctx.eval_count(Run(**run), p.pressure, p.temperature, p.density).tolist() == ev.tolist()
+        _, g64 = ctx.compute(Run(precision="fp64", **run), p.pressure, p.temperature, p.density,
+                             want64=True)
+        err, n = rel_err(g64, ref, 0.0)
+        assert err <= FP64_TOL, err
+        del g64
+        g32 = ctx.compute(Run(precision="fp32c", **run), p.pressure, p.temperature, p.density)
+    m = ref > 1e-6 * ref.max()
+    raw = np.abs(g32.astype(np.float64)[m] - ref[m]) / ref[m]
+    e32, n_taint = check_fp32c(g32, ref, orc, tol=FP32C_TOL)
+    print(f"\nfull Venus: FP64 max rel err {err:.3e}; FP32c max rel err {raw.max():.3e} over "
+          f"{m.sum()} significant points, {int((raw > FP32C_TOL).sum())} above 1e-5, "
+          f"{n_taint} below cascade near-ties, max outside them {e32:.3e}")
+    assert e32 <= FP32C_TOL
+    assert n_taint <= 1e-6 * ref.size
