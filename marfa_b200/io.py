@@ -19,6 +19,7 @@ written by one program are read by the other:
 from __future__ import annotations
 
 import os
+import shutil
 from pathlib import Path
 
 import numpy as np
@@ -185,6 +186,48 @@ def read_pt_table(path, v1: float, v2: float):
             wv.append((RECORD_SPAN * rec + np.arange(NT) * step).astype(np.float32))
             vals.append(data.astype(np.float32))
     return np.concatenate(wv), np.concatenate(vals)
+
+
+CONVERTED_DIRECTORY = Path("output") / "processedData"   # handlers/constants.py
+
+
+def read_info(directory) -> dict:
+    """The run parameters a converter needs from info.txt: start and end
+    wavenumber and the molecule (handlers/convert.py:28-40)."""
+    v1 = v2 = molecule = None
+    with open(Path(directory) / "info.txt") as info:
+        for line in info.readlines():
+            if line.startswith("Start Wavenumber"):
+                v1 = float(line.split(":")[1])
+            if line.startswith("End Wavenumber"):
+                v2 = float(line.split(":")[1])
+            if line.startswith("Input Molecule"):
+                molecule = line.split(":")[1]
+    if v1 is None or v2 is None:
+        raise ValueError("Corrupted info file: start or end wavenumbers are not defined")
+    return {"start": v1, "end": v2, "molecule": molecule}
+
+
+def convert_pt_table(directory, level: int, out_directory=None) -> Path:
+    """Restatement of convert_pttable (handlers/convert.py:12-53): the PT
+    table of `level` in a run directory as text.  The output file
+    `<molecule>_<int(v1)>-<int(v2)>_<level>level.dat` in `out_directory`
+    (default output/processedData, relative to the working directory) starts
+    with a copy of info.txt, followed by one line per point,
+    '%15.5f %17.7e' of (wavenumber, value) as float32 (handlers/parsers.py:17-65
+    gives the points).  Returns the path of the written file."""
+    directory = Path(directory)
+    info = read_info(directory)
+    v1, v2 = info["start"], info["end"]
+    wv, vals = read_pt_table(directory / pt_name(level), v1, v2)
+    out_dir = Path(out_directory) if out_directory is not None else CONVERTED_DIRECTORY
+    out = out_dir / f"{info['molecule'].strip()}_{int(v1)}-{int(v2)}_{level}level.dat"
+    shutil.copyfile(directory / "info.txt", out)
+    with open(out, "a") as f:
+        # the same conversions as the reference's f-string on numpy float32:
+        # each value widened to a Python float, then formatted
+        f.write("".join(f"{w:15.5f} {a:17.7e}\n" for w, a in zip(wv.tolist(), vals.tolist())))
+    return out
 
 
 def write_info(directory: Path, molecule, start, end, cutoff, target, profile) -> None:

@@ -100,3 +100,39 @@ def test_profile_roundtrip_and_errors(tmp_path):
     with pytest.raises(MarfaFormatError) as e:
         read_profile(f)
     assert e.value.code == 7
+
+
+def test_pt_reader_and_converter_match_reference_handlers(tmp_path):
+    """The reader and the text converter against golden vectors that the
+    reference's own handlers (parsers.base_parser, convert.convert_pttable)
+    produced for the same run directory (tests/golden/make_pt_golden.py):
+    wavenumbers and values bit for bit, the converted text byte for byte, and
+    the reference's error for a range beyond the file."""
+    import hashlib
+    import json
+    import sys
+    sys.path.insert(0, str(GOLDEN))
+    from make_pt_golden import make_run
+    from marfa_b200.io import convert_pt_table
+    gold = json.loads((GOLDEN / "pt_convert.json").read_text())
+    sha = lambda b: hashlib.sha256(b).hexdigest()
+    run = tmp_path / "run"
+    run.mkdir()
+    make_run(run)
+    level = gold["run"]["level"]
+    assert sha((run / pt_name(level)).read_bytes()) == gold["ptbin_sha256"]
+    for case in gold["cases"]:
+        if "index_error" in case:
+            with pytest.raises(IndexError) as e:
+                read_pt_table(run / pt_name(level), case["v1"], case["v2"])
+            assert str(e.value) == case["index_error"]
+            continue
+        wv, vals = read_pt_table(run / pt_name(level), case["v1"], case["v2"])
+        assert len(wv) == case["points"]
+        assert sha(wv.astype(np.float32).tobytes()) == case["wv_sha256"]
+        assert sha(vals.astype(np.float32).tobytes()) == case["values_sha256"]
+    out = tmp_path / "processed"
+    out.mkdir()
+    txt = convert_pt_table(run, level, out)
+    assert txt.name == gold["converted_name"]
+    assert sha(txt.read_bytes()) == gold["converted_sha256"]
