@@ -33,8 +33,7 @@ struct DevBuf {
 // Launch parameters that do not change results (chosen by marfa_autotune).
 struct Tune {
   int far_chunk = 16384;   // lines per far-kernel block
-  int coop_k = 5;          // fine grids whose sites are summed by lane groups
-  int sparse_lines = 1024; // units with fewer near lines skip untouched sites
+  int coop_k = 5;          // fine grids whose cell pairs are summed by lane groups
   int small_block_lines = 512; // batches whose units all have fewer near lines use small blocks
 };
 
@@ -846,15 +845,6 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.c = cst;
     fn.scratch = B.scr->p;
     fn.err = ctx->d_err;
-    fn.phase_clock = nullptr;
-    // diagnostics: MARFA_PHASE_CLOCK=<file> records clock64 marks of every
-    // fine-kernel block of the first batch (int64 [units][PHASE_SLOTS]) into <file>
-    const char *clock_path = std::getenv("MARFA_PHASE_CLOCK");
-    if (clock_path && l0 == 0 && !o.graph) {
-      CK(ensure(ctx, ctx->b_count, (size_t)units * PHASE_SLOTS * 8), "alloc clock");
-      CK(cudaMemsetAsync(ctx->b_count.p, 0, (size_t)units * PHASE_SLOTS * 8, cs), "memset clock");
-      fn.phase_clock = (long long *)ctx->b_count.p;
-    }
     const FineChunk &fc = fchunks[c];
     const int max_near = fc.max_near;
     fn.smem_cap = fc.smem_cap;
@@ -869,7 +859,6 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.vbuf = B.vbuf->p;
     fn.queue = (int *)B.queue->p;
     fn.coop_k = ctx->tune.coop_k;
-    fn.sparse_lines = ctx->tune.sparse_lines;
     const int UBc = UB;
     for (int u0 = 0; u0 < units; u0 += UBc) {
       const int nu_ = std::min(UBc, units - u0);
@@ -881,16 +870,6 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       if (f0) cudaEventRecord(f0, cs);
       CK(cudaMemsetAsync(fn.queue, 0, sizeof(int), cs), "memset queue");
       CK(launch_fine(fn, run->precision, chi, cs), "fine kernel");
-      if (fn.phase_clock) {
-        std::vector<long long> pcv((size_t)nu_ * PHASE_SLOTS);
-        CK(cudaMemcpyAsync(pcv.data(), fn.phase_clock, pcv.size() * 8, cudaMemcpyDeviceToHost, cs), "d2h clock");
-        CK(cudaStreamSynchronize(cs), "sync clock");
-        if (FILE *f = std::fopen(clock_path, "wb")) {
-          std::fwrite(pcv.data(), 8, pcv.size(), f);
-          std::fclose(f);
-        }
-        fn.phase_clock = nullptr;
-      }
       ctx->launches += 1;
       if (f1) cudaEventRecord(f1, cs);
       if (adj) {

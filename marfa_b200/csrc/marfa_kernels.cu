@@ -143,9 +143,10 @@ __global__ void __launch_bounds__(256) scatter_kernel(SortParams p) {
 }
 
 // ------------------------------------------------------------ block reduce
+// Sum of v over the block (warp shuffles, then warp partials in `red` in
+// warp order) stored to dst[0 .. N).
 template <int N>
-__device__ __forceinline__ void block_reduce_store(double (&v)[N], double *dst) {
-  __shared__ double red[32][N];
+__device__ __forceinline__ void block_reduce_store(double (&v)[N], double *dst, double (*red)[N]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int k = 0; k < N; ++k) {
@@ -439,7 +440,8 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
     }
     fa.store(res);
   }
-  block_reduce_store<NFAR>(res, p.out + ((size_t)l * p.n_chunks + ci) * NFAR);
+  __shared__ double red[32][NFAR];
+  block_reduce_store<NFAR>(res, p.out + ((size_t)l * p.n_chunks + ci) * NFAR, red);
 }
 
 // --------------------------------------------------------------- near lines
@@ -511,30 +513,16 @@ struct NearStore {
     }
     return voigt_core<Real, CHI>(X, qxv, vy[q], lorA[q], g2[q], hum[q], lv.perrin_b1, lv.perrin_b2, sqrt14);
   }
-  // first[b] = first centre line with floor(UU * 2^9) >= b, b = 0 .. NBIN9
-  const unsigned short *first;
   // centre lines: floor(UU * 2^11) and floor(V * 2^11), V = fl(10 - UU); the
   // bin of grid k is the value shifted right by 11 - k
   const short *n11, *nv11;
-  // first centre line with UU >= a H_k (bin_k >= a); exact for grids 1..9,
-  // the finest bins (k = 11) scan within one grid-9 bin
-  __device__ __forceinline__ int lbL(int k, int a) const {
-    if (k <= 9) return first[min(a << (9 - k), NBIN9)];
-    int q = first[min(a >> 2, NBIN9)];
-    while (q < c1 && n11[q] < a) ++q;
-    return q;
-  }
-  // first centre line with V < a H_k (V bin_k < a), k <= 9: those lines have
-  // UU > 10 - a H_k; the scan starts one grid-9 bin earlier, which covers the
-  // rounding of V
-  __device__ __forceinline__ int lbV(int k, int a) const {
-    int b = NBIN9 - (a << (9 - k)) - 1;
-    b = b < 0 ? 0 : (b > NBIN9 ? NBIN9 : b);
-    int q = first[b];
-    const int sh = 11 - k;
-    while (q < c1 && (nv11[q] >> sh) >= a) ++q;
-    return q;
-  }
+  // firstU[b] (b = 0 .. NBIN9): first centre line whose grid-9 bin of UU is
+  // >= b; firstV[b] (b = 0 .. NBIN9 + 1): first centre line whose grid-9 bin
+  // of V is < b (V falls along the sorted lines).  The lines of any run of
+  // bins of any grid, in UU or in V, are one index range read off these.
+  const unsigned short *firstU, *firstV;
+  __device__ __forceinline__ int bin_u(int b) const { return firstU[min(b, NBIN9)]; }
+  __device__ __forceinline__ int bin_v(int b) const { return firstV[min(b, NBIN9 + 1)]; }
 };
 
 
@@ -615,15 +603,17 @@ __device__ __forceinline__ double group_sum(double v) {
 //              slot buffer (shared memory when it fits, else an L2-resident
 //              per-block slice), slot = position of the cell relative to
 //              the line.
-//   site half  one thread (a warp on the coarse grids) per accumulator sums
-//              the values of its contiguous runs of lines, in line order.
-// Both halves apply the same placement conditions (derived from
-// LineGridCalc.f90:7-674), from the line's side and from the site's side,
-// as integer comparisons of the lines' bins: with n = floor(UU / H_k) and W
-// an integer, UU >= a H_k <=> n >= a and UU < W H_k <=> n < W (likewise for
-// V = fl(10 - UU) and its bin).  Per accumulator the order of summation is:
-// centre lines of the left walk, centre lines of the right walk, near-left
-// lines, near-right lines, each in ascending shifted-centre order.
+//   site half  every value the line half wrote has exactly one owner: the
+//              cell pair of grid k (or the four finest points of a grid-9
+//              cell) it lands on.  One thread (a lane group on the coarse
+//              grids) per owner sums the values of the owner's runs of
+//              lines, each value once, in line order.
+// The line half applies the placement conditions (derived from
+// LineGridCalc.f90:7-674) as integer comparisons of the lines' bins: with
+// n = floor(UU / H_k) and W an integer, UU >= a H_k <=> n >= a and
+// UU < W H_k <=> n < W (likewise for V = fl(10 - UU) and its bin).  The site
+// half needs no condition: which slots a line wrote and where they land
+// depend only on the parity of its bin (see pair_cells).
 // threads per block: 1024 in the FP32 form (64 registers), 512 in FP64
 __host__ __device__ constexpr int fine_threads(bool f64) { return f64 ? 512 : 1024; }
 __device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
@@ -651,6 +641,12 @@ struct LineEval {
     B1 = (Real)0.5641896 * Y;
     A2 = (Real)0.25 + Y2 + Y2 * Y2;
     B2 = Y2 + Y2 - (Real)1.;
+    // regions 2 and 3 need VX + VY < 15 (< 5.5), so VY below that bound: a
+    // line with a larger VY never selects their coefficients
+    const Real z = (Real)0;
+    A3 = B3 = C3 = D3 = A4 = B4 = C4 = D4 = z;
+    A5 = B5 = C5 = D5 = E5 = A6 = B6 = C6 = D6 = E6 = z;
+    if (vy >= 15.0) return;
     A3 = Y * horner<Real>(Y2, 0.56419, 3.10304, 4.65456, 1.05786);
     B3 = Y * horner<Real>(Y2, 1.69257, 0.56419, 2.962);
     C3 = Y * ((Real)1.69257 * Y2 - (Real)2.53885);
@@ -659,6 +655,7 @@ struct LineEval {
     B4 = horner<Real>(Y2, 4.0, 6.0, 9.0, -4.5);
     C4 = (Real)10.5 + (Real)6.0 * (Y2 - (Real)1.0) * Y2;
     D4 = (Real)4.0 * Y2 - (Real)6.0;
+    if (vy >= 5.5) return;
     A5 = horner<Real>(Y, 0.564224, 7.55895, 49.5213, 204.510, 581.746, 1174.8, 1678.33, 1629.76, 973.778,
                       272.102);
     B5 = horner<Real>(Y, 2.25689, 22.6778, 100.705, 247.198, 336.364, 220.843, -2.34403, -60.5644);
@@ -748,8 +745,7 @@ __device__ __forceinline__ double i2d(int n) {
 // The offsets X are exact: UU - e H_k is a multiple of the ulp of UU not
 // larger than UU, and so are its neighbours e -+ 1 built from it.
 template <bool F64, int CHI>
-__device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearStore<F64>::Real *vb, int cap,
-                          unsigned *touched) {
+__device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearStore<F64>::Real *vb, int cap) {
   // Every offset of the line half is below 3 cm-1 in magnitude (at most
   // 4.5 H_k for centre lines, 2 H_{k-1} for near lines, k >= 1), where each
   // chi factor is exactly 1 (ChiFactors.f90: the factors start at |X| = 3):
@@ -757,66 +753,49 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
   LineEval<F64, CHI_NONE> ev;
   const double UU = st.uu[q];
   const int cls = q < st.c0 ? 0 : (q < st.c1 ? 1 : 2);
-  // value of slot `slot` at offset X; `site` is marked as touched when the
-  // unit keeps a touched-site map (sites of grid k: cell e -> e for its edge
-  // e and its mid e; finest point i -> i - 2)
+  // value of slot `slot` at offset X (`site`, the edge / mid / finest point
+  // the slot stands for, documents the placement: grid k cell e -> e for its
+  // edge e and its mid e; finest point i -> i - 2)
   auto put = [&](int slot, int site, double X) {
+    (void)site;
     vb[(size_t)slot * cap + q] = ev(X, st.lv, st.sqrt14);
-    if (touched) atomicOr(touched + (site >> 5), 1u << (site & 31));
   };
   if (k <= 9) {
     const double hk = h_k(k), hk1 = h_k(k - 1), hn = h_k(k + 1);
     const int ntk = nt_k(k);
     if (cls == 1) {
+      // The walk conditions (LineGridCalc.f90:202-331, 343-484) reduce to the
+      // parity of the bins: a line of left bin n >= 2 walks edge n-1 (slot 0),
+      // edge n-2 (slot 1) and mid n-1 (slot 3), and for odd n also edge n-3
+      // (slot 2) and mid n-2 (slot 4); the right walk likewise with its bin
+      // nv (slots 5..9).  Equal to the per-cell rules L(e): e >= 1,
+      // UU < (2 floor((e+1)/2) + 2) H_k, P(e+1): UU >= (e+2) H_k, ... for
+      // every bin of every grid.
       const int n = st.n11[q] >> (11 - k);
       const int nv = st.nv11[q] >> (11 - k);
-      const double V = DELTA_WV - UU;
-      const double bL = UU - i2d(n - 1) * hk; // X of edge n-1
-      const double bV = V - i2d(nv - 1) * hk; // X of the right-walk edge with rP = nv-1
-      bool any = false;
-      bool te[3], tm[2], re[3], rm[2];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) { // left walk, edge e = n-1-d: L(e) and/or P(e+1)
-        const int e = n - 1 - d;
-        const bool tl = e >= 1 && e <= ntk && n < 2 * ((e + 1) / 2) + 2;
-        const bool tp = e >= 0 && e <= ntk - 1 && d >= 1 && n < 2 * ((e + 2) / 2) + 2;
-        te[d] = tl || tp;
-        any |= te[d];
-      }
-#pragma unroll
-      for (int d = 0; d < 2; ++d) { // left walk, mid m = n-1-d
-        const int m = n - 1 - d;
-        tm[d] = m >= 1 && m <= ntk && n < 2 * ((m + 1) / 2) + 2;
-        any |= tm[d];
-      }
-#pragma unroll
-      for (int d = 0; d < 3; ++d) { // right walk, edge e = ntk-nv+1+d (rP = nv-1-d, rL = rP+1)
-        const int e = ntk - nv + 1 + d, rP = nv - 1 - d, rL = rP + 1;
-        const bool tl = e >= 1 && e <= ntk && nv >= rL + 1 && nv < 2 * ((rL + 1) / 2) + 2;
-        const bool tp = e >= 0 && e <= ntk - 1 && nv < 2 * ((rP + 1) / 2) + 2;
-        re[d] = tl || tp;
-        any |= re[d];
-      }
-#pragma unroll
-      for (int d = 0; d < 2; ++d) { // right walk, mid m = ntk+2-nv+d (r = nv-1-d)
-        const int m = ntk + 2 - nv + d, r = nv - 1 - d;
-        rm[d] = m >= 1 && m <= ntk && nv < 2 * ((r + 1) / 2) + 2;
-        any |= rm[d];
-      }
-      if (!any) return;
+      if (n < 2 && nv < 2) return;
       ev.init(st, q);
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-        if (te[d]) put(d, n - 1 - d, bL + (double)d * hk);
-#pragma unroll
-      for (int d = 0; d < 2; ++d)
-        if (tm[d]) put(3 + d, n - 1 - d, (bL + (double)d * hk) + hn);
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-        if (re[d]) put(5 + d, ntk - nv + 1 + d, bV + (double)d * hk);
-#pragma unroll
-      for (int d = 0; d < 2; ++d)
-        if (rm[d]) put(8 + d, ntk + 2 - nv + d, (bV + (double)d * hk) + hn);
+      if (n >= 2) {
+        const double bL = UU - i2d(n - 1) * hk; // X of edge n-1
+        put(0, n - 1, bL);
+        put(1, n - 2, bL + hk);
+        put(3, n - 1, bL + hn);
+        if (n & 1) {
+          put(2, n - 3, bL + 2.0 * hk);
+          put(4, n - 2, (bL + hk) + hn);
+        }
+      }
+      if (nv >= 2) {
+        const double V = DELTA_WV - UU;
+        const double bV = V - i2d(nv - 1) * hk; // X of the right-walk edge ntk-nv+1
+        put(5, ntk - nv + 1, bV);
+        put(6, ntk - nv + 2, bV + hk);
+        put(8, ntk - nv + 2, bV + hn);
+        if (nv & 1) {
+          put(7, ntk - nv + 3, bV + 2.0 * hk);
+          put(9, ntk - nv + 3, (bV + hk) + hn);
+        }
+      }
     } else if (cls == 0) {
       if (UU > -hk1) { // D = -UU < H_{k-1}: cells 1 and 2 (leftLBL labels 20-28, 121-129)
         ev.init(st, q);
@@ -876,121 +855,110 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
   }
 }
 
-__device__ __forceinline__ bool is_touched(const unsigned *touched, int site) {
-  return (touched[site >> 5] >> (site & 31)) & 1u;
-}
-
-// The site half reads the slot values of up to GB lines per batch, loads
-// first, sums after, so that the loads of a batch are in flight together.
-constexpr int GB = 2;
-
-// Site half: cell e (0..ntk) of grid k -> L(e), P(e+1) of edge e and M(e) of
-// mid e.  The mid takes exactly the lines that give L(e) (its walk conditions
-// are those of L(e), at offset X + H_{k+1}), so one pass over the edge's line
-// runs serves all three accumulators.  Lanes of a warp stride over the lines
-// when stride > 1: a group of `stride` lanes (aligned within the warp) sums
-// one cell and its first lane stores the sums.  Every lane of the warp calls
-// this the same number of times (the group sum shuffles); a group whose cell
-// lies past the grid (e > ntk) takes no lines and stores nothing.
-template <bool F64, int stride>
-__device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typename NearStore<F64>::Real *vb,
-                            int cap, void *scr, int lane) {
+// ------------------------------------------------------------ site half
+// Cell pair p of grid k: cells A = 2p - 1 and B = 2p (p = 1 .. ntk / 2).
+// From the walk conditions (LineGridCalc.f90:202-331 left, :343-484 right,
+// as line_pass restates them), a centre line of left bin n walks only the
+// pair floor(n / 2), and a centre line of right bin nv only the pair
+// ntk / 2 + 1 - floor(nv / 2); which slots it wrote and the accumulators they
+// land on depend only on the parity of the bin (c = ntk / 2 + 1 - p):
+//   left,  n  = 2p     : L_A s0, P_A s1, M_A s3
+//   left,  n  = 2p + 1 : L_B s0, P_B s1, M_B s3, L_A s1, P_A s2, M_A s4
+//   right, nv = 2c + 1 : P_A s5, L_A s6, M_A s8, P_B s6, L_B s7, M_B s9
+//   right, nv = 2c     : P_B s5, L_B s6, M_B s8
+// (P(j), L(j): left / right edge of cell j, the edge values L(e) and
+// P(e + 1) being one value.)  Near-left lines with D < H_{k-1} reach pair 1,
+// near-right lines with U < H_{k-1} pair ntk / 2; `own` is D >= H_k (U >= H_k):
+//   near-left : own: P_A s0, L_A s1, M_A s3;  all: P_B s1, L_B s2, M_B s4
+//   near-right: own: L_B s0, M_B s3, P_B s1;  all: L_A s1, M_A s4, P_A s2
+// Lines sorted by shifted centre have n rising and nv falling, so each of the
+// four bin runs is one index range.  G lanes share a pair: they stride over
+// the runs, then a fixed-order group reduction; every lane of the warp calls
+// this the same number of times, and a group whose p lies past the grid sums
+// nothing and stores nothing.
+template <bool F64, int G>
+__device__ void pair_cells(const NearStore<F64> &st, int k, int p, const typename NearStore<F64>::Real *vb,
+                           int cap, typename NearStore<F64>::Real *scr, int lane) {
   using Real = typename NearStore<F64>::Real;
-  const double hk = h_k(k), hk1 = h_k(k - 1);
-  const int ntk = nt_k(k), sh = 11 - k;
-  const bool valid = e <= ntk;
-  const bool hasL = e >= 1, hasP = e <= ntk - 1; // hasL is also "has M"
-  const int wl = 2 * ((e + 1) / 2) + 2, wp = 2 * ((e + 2) / 2) + 2; // walk ends of e, e+1 in bins
-  Acc<F64> aL, aP, aM;
-  aL.init();
-  aP.init();
-  aM.init();
-  Real f[GB], g[GB];
-  bool tl[GB], tp[GB];
-  auto flush = [&]() {
-#pragma unroll
-    for (int j = 0; j < GB; ++j) {
-      if (tl[j]) {
-        aL.add(f[j]);
-        aM.add(g[j]);
-      }
-      if (tp[j]) aP.add(f[j]);
+  const int ntk = nt_k(k), np = ntk >> 1, sh = 9 - k;
+  const bool valid = p <= np;
+  Acc<F64> PA, MA, LA, PB, MB, LB;
+  PA.init(); MA.init(); LA.init(); PB.init(); MB.init(); LB.init();
+  if (valid) {
+    const Real *v0 = vb, *v1 = vb + cap, *v2 = vb + 2 * (size_t)cap, *v3 = vb + 3 * (size_t)cap,
+               *v4 = vb + 4 * (size_t)cap;
+    const int q0 = st.bin_u((2 * p) << sh), q1 = st.bin_u((2 * p + 1) << sh), q2 = st.bin_u((2 * p + 2) << sh);
+    for (int q = q0 + lane; q < q1; q += G) {
+      LA.add(v0[q]);
+      PA.add(v1[q]);
+      MA.add(v3[q]);
     }
-  };
-  { // left walk: bins e+1 .. e+3
-    const int q0 = valid ? st.lbL(k, e + 1) : 0, q1 = valid ? st.lbL(k, e + 4) : 0;
-    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        const int n = q < q1 ? st.n11[q] >> sh : -1;
-        tl[j] = hasL && n >= e + 1 && n < wl;
-        tp[j] = hasP && n >= e + 2 && n < wp;
-        f[j] = (tl[j] || tp[j]) ? vb[(size_t)(n - 1 - e) * cap + q] : (Real)0;
-        g[j] = tl[j] ? vb[(size_t)(3 + n - 1 - e) * cap + q] : (Real)0;
-      }
-      flush();
+    for (int q = q1 + lane; q < q2; q += G) {
+      const Real f1 = v1[q];
+      LB.add(v0[q]);
+      PB.add(f1);
+      MB.add(v3[q]);
+      LA.add(f1);
+      PA.add(v2[q]);
+      MA.add(v4[q]);
     }
-  }
-  { // right walk: V bins ntk-e+1 .. ntk-e+3
-    const int rL = ntk + 1 - e, rP = ntk - e;
-    const int wrl = 2 * ((rL + 1) / 2) + 2, wrp = 2 * ((rP + 1) / 2) + 2;
-    const int q0 = valid ? st.lbV(k, ntk - e + 4) : 0, q1 = valid ? st.lbV(k, ntk - e + 1) : 0;
-    for (int qb = q0 + lane; qb < q1; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        const int nv = q < q1 ? st.nv11[q] >> sh : -1;
-        tl[j] = hasL && nv >= rL + 1 && nv < wrl;
-        tp[j] = hasP && nv >= rP + 1 && nv < wrp;
-        f[j] = (tl[j] || tp[j]) ? vb[(size_t)(5 + e - (ntk - nv + 1)) * cap + q] : (Real)0;
-        g[j] = tl[j] ? vb[(size_t)(8 + e - (ntk + 2 - nv)) * cap + q] : (Real)0;
-      }
-      flush();
+    const Real *v5 = vb + 5 * (size_t)cap, *v6 = vb + 6 * (size_t)cap, *v7 = vb + 7 * (size_t)cap,
+               *v8 = vb + 8 * (size_t)cap, *v9 = vb + 9 * (size_t)cap;
+    const int c = np + 1 - p;
+    const int r0 = st.bin_v((2 * c + 2) << sh), r1 = st.bin_v((2 * c + 1) << sh), r2 = st.bin_v((2 * c) << sh);
+    for (int q = r0 + lane; q < r1; q += G) {
+      const Real f6 = v6[q];
+      PA.add(v5[q]);
+      LA.add(f6);
+      MA.add(v8[q]);
+      PB.add(f6);
+      LB.add(v7[q]);
+      MB.add(v9[q]);
     }
-  }
-  if (valid && e <= 2) { // near-left lines with D < H_{k-1}
-    const int q0 = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
-    for (int qb = q0 + lane; qb < st.c0; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        const bool in = q < st.c0;
-        const bool own = in && -st.uu[q] >= hk;
-        tl[j] = in && ((e == 1 && own) || e == 2);
-        tp[j] = in && ((e == 0 && own) || e == 1);
-        f[j] = (tl[j] || tp[j]) ? vb[(size_t)e * cap + q] : (Real)0;
-        g[j] = tl[j] ? vb[(size_t)(2 + e) * cap + q] : (Real)0;
-      }
-      flush();
+    for (int q = r1 + lane; q < r2; q += G) {
+      PB.add(v5[q]);
+      LB.add(v6[q]);
+      MB.add(v8[q]);
     }
-  }
-  if (valid && e >= ntk - 2) { // near-right lines with U < H_{k-1}
-    const int q1 = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
-    for (int qb = st.c1 + lane; qb < q1; qb += GB * stride) {
-#pragma unroll
-      for (int j = 0; j < GB; ++j) {
-        const int q = qb + j * stride;
-        const bool in = q < q1;
-        const bool own = in && (st.uu[q] - DELTA_WV) >= hk;
-        tl[j] = in && ((e == ntk && own) || e == ntk - 1);
-        tp[j] = in && ((e == ntk - 1 && own) || e == ntk - 2);
-        f[j] = (tl[j] || tp[j]) ? vb[(size_t)(ntk - e) * cap + q] : (Real)0;
-        g[j] = tl[j] ? vb[(size_t)(3 + ntk - e) * cap + q] : (Real)0;
+    if (p == 1) { // near-left lines with D < H_{k-1}, ascending UU: own (D >= H_k) first
+      const double hk = h_k(k), hk1 = h_k(k - 1);
+      const int qn = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -hk1; });
+      for (int q = qn + lane; q < st.c0; q += G) {
+        if (-st.uu[q] >= hk) {
+          PA.add(v0[q]);
+          LA.add(v1[q]);
+          MA.add(v3[q]);
+        }
+        PB.add(v1[q]);
+        LB.add(v2[q]);
+        MB.add(v4[q]);
       }
-      flush();
+    }
+    if (p == np) { // near-right lines with U < H_{k-1}, ascending U: own (U >= H_k) last
+      const double hk = h_k(k), hk1 = h_k(k - 1);
+      const int qn = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= hk1; });
+      for (int q = st.c1 + lane; q < qn; q += G) {
+        if ((st.uu[q] - DELTA_WV) >= hk) {
+          LB.add(v0[q]);
+          MB.add(v3[q]);
+          PB.add(v1[q]);
+        }
+        LA.add(v1[q]);
+        MA.add(v4[q]);
+        PA.add(v2[q]);
+      }
     }
   }
-  const double vL = group_sum<stride>(aL.value()), vP = group_sum<stride>(aP.value());
-  const double vM = group_sum<stride>(aM.value());
+  const double pa = group_sum<G>(PA.value()), ma = group_sum<G>(MA.value()), la = group_sum<G>(LA.value());
+  const double pb = group_sum<G>(PB.value()), mb = group_sum<G>(MB.value()), lb = group_sum<G>(LB.value());
   if (valid && lane == 0) {
-    Real *o = (Real *)scr;
-    const int cb = base_k(k) - NT0;
-    if (hasL) {
-      o[SCR_FINE_L + cb + e - 1] = (Real)vL;
-      o[SCR_FINE_M + cb + e - 1] = (Real)vM;
-    }
-    if (hasP) o[SCR_FINE_P + cb + e] = (Real)vP;
+    const int a = base_k(k) - NT0 + 2 * p - 2; // cell A; cell B follows
+    scr[SCR_FINE_P + a] = (Real)pa;
+    scr[SCR_FINE_M + a] = (Real)ma;
+    scr[SCR_FINE_L + a] = (Real)la;
+    scr[SCR_FINE_P + a + 1] = (Real)pb;
+    scr[SCR_FINE_M + a + 1] = (Real)mb;
+    scr[SCR_FINE_L + a + 1] = (Real)lb;
   }
 }
 
@@ -999,30 +967,27 @@ __device__ void gather_cell(const NearStore<F64> &st, int k, int e, const typena
 // (4 floor((i-2)/4) + 8) H = (4j + 4) H and the right fine loop's V bound is
 // (floor((NT-i)/4) + 2) H9 = (5122 - j) H9, so every line of the run
 // [first V < (5122 - j) H9, first UU >= (4j + 4) H) reaches all four points:
-// point i through its left loop when floor(UU/H) >= i - 1, else through its
-// right loop.  Per point, the left-loop lines are summed first, then the
-// right-loop lines, then the near lines (the order of the point form).
+// point i through its left loop (slot floor(UU/H) + 1 - i) when
+// floor(UU/H) >= i - 1, else through its right loop (slot
+// 7 + i - floor(UU/H) - 2).  Then the near lines: RK(2..5) from the near-left
+// lines with D < H9, RK(NT-3..NT) from the near-right lines with U < H9.
 template <bool F64>
-__device__ void gather_quad(const NearStore<F64> &st, int j, const typename NearStore<F64>::Real *vb, int cap,
-                            void *scr) {
-  using Real = typename NearStore<F64>::Real;
+__device__ void quad_points(const NearStore<F64> &st, int j, const typename NearStore<F64>::Real *vb, int cap,
+                            typename NearStore<F64>::Real *scr) {
   const double H9 = h_k(9);
   const int i0 = 4 * j - 2;
   Acc<F64> a[4];
 #pragma unroll
   for (int p = 0; p < 4; ++p) a[p].init();
-  const int q0 = st.lbV(9, 5122 - j), q1 = st.lbL(11, 4 * j + 4);
-  for (int q = q0; q < q1; ++q) { // left fine loops
+  const int q0 = st.bin_v(5122 - j), q1 = st.bin_u(j + 1);
+  for (int q = q0; q < q1; ++q) {
     const int ni = st.n11[q];
 #pragma unroll
-    for (int p = 0; p < 4; ++p)
-      if (ni >= i0 + p - 1) a[p].add(vb[(size_t)(ni + 1 - i0 - p) * cap + q]);
-  }
-  for (int q = q0; q < q1; ++q) { // right fine loops
-    const int ni = st.n11[q];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-      if (ni < i0 + p - 1) a[p].add(vb[(size_t)(7 + i0 + p - ni - 2) * cap + q]);
+    for (int p = 0; p < 4; ++p) {
+      const int i = i0 + p;
+      const int slot = ni >= i - 1 ? ni + 1 - i : 5 + i - ni;
+      a[p].add(vb[(size_t)slot * cap + q]);
+    }
   }
   if (j == 1) { // RK(2..5): near-left lines with D < H9
     const int qn = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -H9; });
@@ -1036,9 +1001,8 @@ __device__ void gather_quad(const NearStore<F64> &st, int j, const typename Near
 #pragma unroll
       for (int p = 0; p < 4; ++p) a[p].add(vb[(size_t)(NT - i0 - p) * cap + q]);
   }
-  Real *o = (Real *)scr;
 #pragma unroll
-  for (int p = 0; p < 4; ++p) o[SCR_RK + i0 + p - 2] = (Real)a[p].value();
+  for (int p = 0; p < 4; ++p) scr[SCR_RK + i0 + p - 2] = (typename NearStore<F64>::Real)a[p].value();
 }
 
 __device__ __forceinline__ int block_excl_scan(int v, int &total) {
@@ -1089,8 +1053,6 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   __syncthreads();
   const int64_t a = sb[0], b = sb[3];
   const int cnt = (int)(b - a);
-  long long *pc = p.phase_clock ? p.phase_clock + (size_t)ub * PHASE_SLOTS : nullptr;
-  if (pc && threadIdx.x == 0) { pc[0] = clock64(); pc[3] = cnt; }
   // staging area: shared memory, or this block's slice of the global staging buffer
   const bool staged_smem = cnt <= p.smem_cap;
   const int cap = staged_smem ? p.smem_cap : p.gstage_cap;
@@ -1156,18 +1118,14 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     __syncthreads();
     return;
   }
-  // grid-9 bin table of the centre lines: entry b is the first line whose
-  // bin is >= b, written by the line that opens the range of bins
-  __shared__ unsigned short s_first[NBIN9 + 1];
-  for (int q = st.c0 + threadIdx.x; q <= st.c1; q += blockDim.x) {
-    const int bq = q < st.c1 ? min(st.n11[q] >> 2, NBIN9) : NBIN9 + 1;
-    const int bp = q > st.c0 ? min(st.n11[q - 1] >> 2, NBIN9) : -1;
-    for (int bb = bp + 1; bb <= min(bq, NBIN9); ++bb) s_first[bb] = (unsigned short)q;
-  }
-  __syncthreads();
-  st.first = s_first;
-
-  if (pc && threadIdx.x == 0) pc[1] = clock64();
+  // grid-9 bin tables of the centre lines, built after grid 0; the block
+  // reduction of grid 0 uses the same shared memory before them
+  __shared__ union {
+    struct {
+      unsigned short u[NBIN9 + 1], v[NBIN9 + 2];
+    } first;
+    double red[32][31];
+  } s_tab;
   // grid 0 and RK(1): one thread per near line, block reduction
   {
     Lane<F64> aR, aP[10], aM[10], aL[10];
@@ -1184,90 +1142,67 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
       v[21 + j] = aL[j].value();
     }
     __shared__ double g0[31];
-    block_reduce_store<31>(v, g0);
+    block_reduce_store<31>(v, g0, s_tab.red);
     __syncthreads();
     if (threadIdx.x < 31) scr[threadIdx.x] = (Real)g0[threadIdx.x];
   }
+  // bins of UU rise and bins of V fall along the sorted lines: firstU[b] for
+  // b in (bin(q-1), bin(q)] and firstV[b] for b in (vbin(q), vbin(q-1)] are
+  // written by line q, so every entry is written once
+  for (int q = st.c0 + threadIdx.x; q <= st.c1; q += blockDim.x) {
+    const int bq = q < st.c1 ? min(st.n11[q] >> 2, NBIN9) : NBIN9 + 1;
+    const int bp = q > st.c0 ? min(st.n11[q - 1] >> 2, NBIN9) : -1;
+    for (int bb = bp + 1; bb <= min(bq, NBIN9); ++bb) s_tab.first.u[bb] = (unsigned short)q;
+    const int vq = q < st.c1 ? st.nv11[q] >> 2 : -1;              // <= NBIN9
+    const int vp = q > st.c0 ? st.nv11[q - 1] >> 2 : NBIN9 + 1;
+    for (int bb = vq + 1; bb <= vp; ++bb) s_tab.first.v[bb] = (unsigned short)q;
+  }
   __syncthreads();
-  if (pc && threadIdx.x == 0) pc[2] = clock64();
+  st.firstU = s_tab.first.u;
+  st.firstV = s_tab.first.v;
 
   // slot buffer: in shared memory behind the staged lines when its rows fit
   // there (units staged in shared memory only), else this block's global slice
   Real *vb_g = (Real *)p.vbuf + (size_t)blockIdx.x * p.vbuf_stride;
   Real *vb_s = (Real *)(fine_smem + (size_t)p.smem_cap * (24 + 3 * sizeof(Real) + 4));
-  // sparse units (few near lines) keep a map of the sites with at least one
-  // contribution in the current pass (bit per site); the site half then
-  // skips the others, which are zero
-  __shared__ unsigned s_touched[(NT + 31) / 32];
-  const bool sparse = st.m < p.sparse_lines;
-  unsigned *touched = sparse ? s_touched : nullptr;
   for (int k = 1; k <= 10; ++k) {
-    if (sparse) {
-      for (int w = threadIdx.x; w < (NT + 31) / 32; w += blockDim.x) s_touched[w] = 0u;
-      __syncthreads();
-    }
     const bool vsm = staged_smem && (k <= 9 ? 10 : NSLOT) <= p.vsm_rows;
     Real *vb = vsm ? vb_s : vb_g;
     const int vcap = vsm ? p.smem_cap : p.vbuf_cap;
-    const long long t0 = pc ? clock64() : 0;
-    for (int q = threadIdx.x; q < st.m; q += blockDim.x) line_pass<F64, CHI>(st, q, k, vb, vcap, touched);
+    for (int q = threadIdx.x; q < st.m; q += blockDim.x) line_pass<F64, CHI>(st, q, k, vb, vcap);
     __syncthreads();
-    const long long t1 = pc ? clock64() : 0;
     if (k <= 9) {
-      const int ntk = nt_k(k), nsite = ntk + 1, cb = base_k(k) - NT0;
-      // lanes per cell on grids 1..coop_k: the largest power of two (at most
-      // a warp) with which all cells are summed in one round (about the same
-      // number of lines per lane on every grid: the lines per cell halve as
-      // the cells double); one thread per cell on the other grids and in
-      // sparse units (few lines per site)
+      const int np = nt_k(k) >> 1;
+      // lanes per cell pair on grids 1..coop_k: the largest power of two (at
+      // most a warp) with which all pairs are summed in one round (about the
+      // same number of lines per lane on every grid: the lines per pair halve
+      // as the pairs double); one thread per pair on the other grids
       int G = 1;
-      if (!sparse && k <= p.coop_k) {
-        const int want = (int)blockDim.x / nsite;
+      if (k <= p.coop_k) {
+        const int want = (int)blockDim.x / np;
         G = want >= 32 ? 32 : want >= 16 ? 16 : want >= 8 ? 8 : want >= 4 ? 4 : want >= 2 ? 2 : 1;
       }
       if (G == 1) {
-        for (int e = threadIdx.x; e < nsite; e += blockDim.x) {
-          if (sparse && !is_touched(s_touched, e)) { // no contribution: zero accumulators
-            if (e >= 1) {
-              scr[SCR_FINE_L + cb + e - 1] = (Real)0;
-              scr[SCR_FINE_M + cb + e - 1] = (Real)0;
-            }
-            if (e <= ntk - 1) scr[SCR_FINE_P + cb + e] = (Real)0;
-            continue;
-          }
-          gather_cell<F64, 1>(st, k, e, vb, vcap, scr, 0);
-        }
+        for (int pp = 1 + threadIdx.x; pp <= np; pp += blockDim.x) pair_cells<F64, 1>(st, k, pp, vb, vcap, scr, 0);
       } else {
         const int lane = threadIdx.x & (G - 1), grp = threadIdx.x / G, ngrp = blockDim.x / G;
-        const int rounds = (nsite + ngrp - 1) / ngrp; // the same for every lane
+        const int rounds = (np + ngrp - 1) / ngrp; // the same for every lane
         for (int r = 0; r < rounds; ++r) {
-          const int e = grp + r * ngrp;
+          const int pp = 1 + grp + r * ngrp;
           switch (G) {
-          case 32: gather_cell<F64, 32>(st, k, e, vb, vcap, scr, lane); break;
-          case 16: gather_cell<F64, 16>(st, k, e, vb, vcap, scr, lane); break;
-          case 8: gather_cell<F64, 8>(st, k, e, vb, vcap, scr, lane); break;
-          case 4: gather_cell<F64, 4>(st, k, e, vb, vcap, scr, lane); break;
-          default: gather_cell<F64, 2>(st, k, e, vb, vcap, scr, lane); break;
+          case 32: pair_cells<F64, 32>(st, k, pp, vb, vcap, scr, lane); break;
+          case 16: pair_cells<F64, 16>(st, k, pp, vb, vcap, scr, lane); break;
+          case 8: pair_cells<F64, 8>(st, k, pp, vb, vcap, scr, lane); break;
+          case 4: pair_cells<F64, 4>(st, k, pp, vb, vcap, scr, lane); break;
+          default: pair_cells<F64, 2>(st, k, pp, vb, vcap, scr, lane); break;
           }
         }
       }
     } else {
-      for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) {
-        if (sparse && ((s_touched[(4 * j - 4) >> 5] >> ((4 * j - 4) & 31)) & 15u) == 0u) {
-#pragma unroll
-          for (int p = 0; p < 4; ++p) scr[SCR_RK + 4 * j - 4 + p] = (Real)0;
-        } else {
-          gather_quad<F64>(st, j, vb, vcap, scr);
-        }
-      }
+      for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) quad_points<F64>(st, j, vb, vcap, scr);
     }
     __syncthreads();
-    if (pc && threadIdx.x == 0) {
-      pc[4 + k] = t1 - t0;
-      pc[14 + k] = clock64() - t1;
-    }
   }
-  if (pc && threadIdx.x == 0) pc[4] = clock64();
 }
 
 // Persistent: every block takes units from the work queue until it is empty

@@ -69,10 +69,6 @@ struct FarParams {
 
 // Rows of the fine kernel's slot buffer (values per staged line; the
 // finest-point pass uses 15).
-// diagnostic clock marks per fine-kernel unit: start, staged, grid 0 done,
-// near count, end, line-half cycles of passes 1..10, site-half cycles of
-// passes 1..10
-constexpr int PHASE_SLOTS = 25;
 constexpr int NSLOT = 15;
 
 struct FineParams {
@@ -94,7 +90,6 @@ struct FineParams {
   int gstage_cap;                // lines per block in gstage
   size_t gstage_bytes;           // bytes per block in gstage
   int *err;
-  long long *phase_clock;        // optional [n_units][PHASE_SLOTS] clock64 marks (diagnostics)
   int *queue;                    // work-queue head (zero before the launch)
   const int *order;              // optional processing order of the units
   void *vbuf;                    // per-block slot buffers in global memory
@@ -102,8 +97,7 @@ struct FineParams {
   int vbuf_cap;                  // lines per slot row in vbuf
   int grid;                      // persistent blocks
   int vsm_rows;                  // slot-buffer rows held in shared memory (0, 10 or NSLOT)
-  int sparse_lines;              // units with fewer staged lines skip untouched sites
-  int coop_k;                    // grids 1..coop_k: lane groups per site in the site half
+  int coop_k;                    // grids 1..coop_k: lane groups per cell pair in the site half
   int block_threads;             // threads per block (fine_block_threads)
 };
 

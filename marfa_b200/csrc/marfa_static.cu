@@ -337,7 +337,6 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   fn.c = c;
   fn.scratch = base + OFF_SCR;
   fn.err = &d_small->err;
-  fn.phase_clock = nullptr;
   fn.gstage = base + OFF_GST;
   fn.gstage_cap = 0;
   fn.gstage_bytes = 0;
@@ -365,7 +364,6 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   fn.grid = 1;
   fn.vsm_rows = 0;
   fn.coop_k = 5;
-  fn.sparse_lines = 1024;
   fn.vbuf = base + OFF_VB;
   fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
   fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
