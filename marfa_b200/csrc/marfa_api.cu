@@ -380,7 +380,8 @@ struct VjpOut {
 
 // Fine-kernel launch plan of one chunk of levels.
 struct FineChunk {
-  int max_near = 0, smem_cap = 0, gstage_cap = 0, block_threads = 0, vsm_rows = 0, resident = 0;
+  int max_near = 0, smem_cap = 0, gstage_cap = 0, block_threads = 0, resident = 0;
+  size_t smem_room = 0;
   size_t gstage_bytes = 0;
 };
 
@@ -646,15 +647,15 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       return set_err(ctx, MARFA_E_CAPACITY, "%d lines within 1 cm-1 of one subinterval (at most 65535)",
                      fc.max_near);
     fc.block_threads = fine_block_threads(run->precision, fc.max_near, ctx->tune.small_block_lines);
-    // on-chip staging up to 4096 (FP64) / 2688 (FP32c) lines, and never past
-    // what the block's shared memory holds beside the kernel's static arrays
+    // on-chip staging up to what the block's shared memory holds beside the
+    // kernel's static arrays (each unit then keeps its slot rows on chip
+    // when they fit beside its own lines)
     int smem_lines = 0;
     CK(fine_smem_lines(run->precision, chi, fc.block_threads, &smem_lines), "fine shared memory");
-    const int smem_max = std::min(f64 ? 4096 : 2688, smem_lines);
-    fc.smem_cap = std::max(128, std::min(smem_max, (fc.max_near + 127) / 128 * 128));
+    fc.smem_cap = std::max(128, std::min(smem_lines, (fc.max_near + 127) / 128 * 128));
     fc.gstage_cap = fc.max_near > fc.smem_cap ? (fc.max_near + 255) / 256 * 256 : 0;
     fc.gstage_bytes = fc.gstage_cap ? fine_smem_bytes(fc.gstage_cap, f64) : 0;
-    CK(fine_plan(run->precision, chi, fc.block_threads, fc.smem_cap, &fc.vsm_rows, &fc.resident), "fine occupancy");
+    CK(fine_plan(run->precision, chi, fc.block_threads, fc.smem_cap, &fc.smem_room, &fc.resident), "fine occupancy");
     gstage_need = std::max(gstage_need, (size_t)fc.resident * fc.gstage_bytes);
     vbuf_need = std::max(vbuf_need, (size_t)fc.resident *
                                         fine_vbuf_elems(std::max(fc.smem_cap, fc.gstage_cap)) * elem);
@@ -673,7 +674,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   std::vector<long long> sig = {Lc, UB, (long long)ctx->alloc_gen};
   sig.insert(sig.end(), lb.begin(), lb.end());
   for (const FineChunk &fc : fchunks)
-    sig.insert(sig.end(), {fc.smem_cap, fc.gstage_cap, fc.block_threads, fc.vsm_rows, fc.resident});
+    sig.insert(sig.end(), {fc.smem_cap, fc.gstage_cap, fc.block_threads, (long long)fc.smem_room, fc.resident});
 
   Staging sg{ctx, st};
   const size_t stage_bytes = 4 * Staging::room((size_t)nsub * 8) + Staging::room((size_t)(nsub + 1) * 4) +
@@ -852,7 +853,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     fn.gstage_bytes = fc.gstage_bytes;
     fn.gstage = fc.gstage_cap ? B.gstage->p : nullptr;
     fn.block_threads = fc.block_threads;
-    fn.vsm_rows = fc.vsm_rows;
+    fn.smem_room = fc.smem_room;
     const int resident = fc.resident;
     fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
     fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);

@@ -163,6 +163,49 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[N], double *dst, 
   }
 }
 
+// Warp sums of 16 values per lane by a butterfly reduce-scatter: at the step
+// of lane bit w a lane keeps one half of its values and receives its partner's
+// copy of that half (w + w/2 + ... + 1 = 15 shuffles, then one across the
+// half-warps); lane L ends with the warp's sum of value L & 15.  The order of
+// the additions is fixed.
+__device__ __forceinline__ double warp_scatter16(double (&a)[16]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int w = 8; w >= 1; w >>= 1) {
+    const bool up = (lane & w) != 0;
+#pragma unroll
+    for (int i = 0; i < w; ++i) {
+      const double send = up ? a[i] : a[i + w];
+      const double keep = up ? a[i + w] : a[i];
+      a[i] = keep + __shfl_xor_sync(0xffffffffu, send, w);
+    }
+  }
+  return a[0] + __shfl_xor_sync(0xffffffffu, a[0], 16);
+}
+
+// Sum over the block of 31 values per thread, stored to dst[0 .. 31): two
+// butterfly halves per warp, then the warp sums in warp order (red: 32 x 32).
+template <typename Real>
+__device__ __forceinline__ void block_reduce31(const Real (&v)[31], double *dst, double (*red)[32]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double a[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) a[i] = (double)v[i];
+  double r = warp_scatter16(a);
+  if (lane < 16) red[warp][lane] = r;
+#pragma unroll
+  for (int i = 0; i < 15; ++i) a[i] = (double)v[16 + i];
+  a[15] = 0.0;
+  r = warp_scatter16(a);
+  if (lane < 15) red[warp][16 + lane] = r;
+  __syncthreads();
+  if (threadIdx.x < 31) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w][threadIdx.x];
+    dst[threadIdx.x] = t;
+  }
+}
+
 // ---------------------------------------------------------------- far lines
 // First grid-0 position index k (0..21) whose distance D + k/2 passes the
 // chi-factor boundary b (strictly when `strict`), decided in double.
@@ -583,23 +626,15 @@ __device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Lane
   }
 }
 
-// Sum over each group of G lanes (G = 1, 2, 4, 8, 16 or 32; the first lane
-// of the group gets the total).  Every lane of the warp takes part.
-template <int G>
-__device__ __forceinline__ double group_sum(double v) {
-#pragma unroll
-  for (int off = G >> 1; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off, G);
-  return v;
-}
-
 // ----------------------------------------------------------- fine grids
-// Grids 1..9 and the direct finest points are computed in ten passes (one
-// per grid, then the finest points).  Each pass has two halves:
+// Grids 1..9 and the direct finest points are computed in eleven passes (one
+// per grid, then the finest points of the left fine loops and of the right
+// fine loops).  Each pass has two halves:
 //   line half  one thread per near line evaluates every cell of the pass's
 //              grid that the line's walk visits (centerLBL, and the fine
 //              parts of leftLBL / rightLBL).  The line's Kuntz coefficients
-//              are computed once per pass; every evaluation picks its
-//              region's set by selects, without branching.  Values go to a
+//              are computed once per pass (regions 2 and 3 only when the
+//              pass's smallest offset can reach them).  Values go to a
 //              slot buffer (shared memory when it fits, else an L2-resident
 //              per-block slice), slot = position of the cell relative to
 //              the line.
@@ -630,7 +665,11 @@ struct LineEval {
   Real A3, B3, C3, D3, A4, B4, C4, D4;         // region 2 (Shapes.f90:72-86)
   Real A5, B5, C5, D5, E5, A6, B6, C6, D6, E6; // region 3 (Shapes.f90:88-113)
 
-  __device__ __forceinline__ void init(const NearStore<F64> &st, int q) {
+  // xlo: a lower bound of |X| over the evaluations that follow.  Regions 2
+  // and 3 need VX + VY < 15 (< 5.5 with VX <= 1 or VY >= 0.02), decided on
+  // the same double values as the evaluation, so their coefficients are
+  // computed only when the smallest VX = xlo * qx can reach them.
+  __device__ __forceinline__ void init(const NearStore<F64> &st, int q, double xlo) {
     qx = st.qx[q];
     vy = st.vy[q];
     lorA = st.lorA[q];
@@ -641,12 +680,11 @@ struct LineEval {
     B1 = (Real)0.5641896 * Y;
     A2 = (Real)0.25 + Y2 + Y2 * Y2;
     B2 = Y2 + Y2 - (Real)1.;
-    // regions 2 and 3 need VX + VY < 15 (< 5.5), so VY below that bound: a
-    // line with a larger VY never selects their coefficients
     const Real z = (Real)0;
     A3 = B3 = C3 = D3 = A4 = B4 = C4 = D4 = z;
     A5 = B5 = C5 = D5 = E5 = A6 = B6 = C6 = D6 = E6 = z;
-    if (vy >= 15.0) return;
+    const double vlo = xlo * qx, slo = vlo + vy;
+    if (qx >= 0.0 && !(slo < 15.0)) return;
     A3 = Y * horner<Real>(Y2, 0.56419, 3.10304, 4.65456, 1.05786);
     B3 = Y * horner<Real>(Y2, 1.69257, 0.56419, 2.962);
     C3 = Y * ((Real)1.69257 * Y2 - (Real)2.53885);
@@ -655,7 +693,7 @@ struct LineEval {
     B4 = horner<Real>(Y2, 4.0, 6.0, 9.0, -4.5);
     C4 = (Real)10.5 + (Real)6.0 * (Y2 - (Real)1.0) * Y2;
     D4 = (Real)4.0 * Y2 - (Real)6.0;
-    if (vy >= 5.5) return;
+    if (qx >= 0.0 && !(slo < 5.5 && (vlo <= 1.0 || vy >= 0.02))) return;
     A5 = horner<Real>(Y, 0.564224, 7.55895, 49.5213, 204.510, 581.746, 1174.8, 1678.33, 1629.76, 973.778,
                       272.102);
     B5 = horner<Real>(Y, 2.25689, 22.6778, 100.705, 247.198, 336.364, 220.843, -2.34403, -60.5644);
@@ -712,25 +750,25 @@ struct LineEval {
       if (sizeof(Real) == 8) return lor * (Real)chi_factor_d<CHI>(ax, lv);
       return lor * (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
     }
+    // Kuntz regions 1-3 (Shapes.f90:63-113): one branch per region (a warp
+    // runs the regions its lanes need; the Horner forms round exactly as the
+    // degree-(4, 5) form with the leading coefficients zero would)
     const double sum = VXd + vy;
-    const bool r1 = sum >= 15.0, r2 = !r1 && sum >= 5.5;
-    if (!r1 && !r2 && !(VXd <= 1.0 || vy >= 0.02)) return region4(ax, VXd, lv, sqrt14);
     const Real VX = (Real)VXd;
     const Real x = VX * VX;
-    const Real z = (Real)0, o = (Real)1;
-    const Real n0 = (r1 || r2) ? z : E5;
-    const Real n1 = r1 ? z : (r2 ? D3 : D5);
-    const Real n2 = r1 ? z : (r2 ? C3 : C5);
-    const Real n3 = r1 ? B1 : (r2 ? B3 : B5);
-    const Real n4 = r1 ? A1 : (r2 ? A3 : A5);
-    const Real d0 = (r1 || r2) ? z : o;
-    const Real d1 = r1 ? z : (r2 ? o : E6);
-    const Real d2 = r1 ? z : (r2 ? D4 : D6);
-    const Real d3 = r1 ? o : (r2 ? C4 : C6);
-    const Real d4 = r1 ? B2 : (r2 ? B4 : B6);
-    const Real d5 = r1 ? A2 : (r2 ? A4 : A6);
-    const Real num = (((n0 * x + n1) * x + n2) * x + n3) * x + n4;
-    const Real den = ((((d0 * x + d1) * x + d2) * x + d3) * x + d4) * x + d5;
+    Real num, den;
+    if (sum >= 15.0) {
+      num = B1 * x + A1;
+      den = (x + B2) * x + A2;
+    } else if (sum >= 5.5) {
+      num = ((D3 * x + C3) * x + B3) * x + A3;
+      den = (((x + D4) * x + C4) * x + B4) * x + A4;
+    } else if (VXd <= 1.0 || vy >= 0.02) {
+      num = (((E5 * x + D5) * x + C5) * x + B5) * x + A5;
+      den = ((((x + E6) * x + D6) * x + C6) * x + B6) * x + A6;
+    } else {
+      return region4(ax, VXd, lv, sqrt14);
+    }
     return fast_div(num, den) * hum;
   }
 };
@@ -774,7 +812,7 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
       const int n = st.n11[q] >> (11 - k);
       const int nv = st.nv11[q] >> (11 - k);
       if (n < 2 && nv < 2) return;
-      ev.init(st, q);
+      ev.init(st, q, hk); // every offset of a centre walk is at least H_k
       if (n >= 2) {
         const double bL = UU - i2d(n - 1) * hk; // X of edge n-1
         put(0, n - 1, bL);
@@ -798,7 +836,7 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
       }
     } else if (cls == 0) {
       if (UU > -hk1) { // D = -UU < H_{k-1}: cells 1 and 2 (leftLBL labels 20-28, 121-129)
-        ev.init(st, q);
+        ev.init(st, q, 0.0);
         const bool own = -UU >= hk;
         if (own) put(0, 0, UU);            // e = 0: P(1)
         put(1, 1, UU - hk);                // e = 1: L(1) when own, P(2)
@@ -809,7 +847,7 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
     } else {
       const double U = UU - DELTA_WV;
       if (U < hk1) { // cells ntk and ntk-1 (rightLBL labels 60-69, 131-139)
-        ev.init(st, q);
+        ev.init(st, q, 0.0);
         const bool own = U >= hk;
         if (own) put(0, ntk, U);               // e = ntk: L(ntk)
         put(1, ntk - 1, U + hk);               // e = ntk-1: L(ntk-1), P(ntk) when own
@@ -819,24 +857,29 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
       }
     }
   } else {
+    // the finest points in two passes: k = 10 the left fine loops and the
+    // near-left lines, k = 11 the right fine loops and the near-right lines
     const double H = HSTEP, H9 = h_k(9);
     if (cls == 1) {
-      ev.init(st, q);
       const int ni = st.n11[q], nv9 = st.nv11[q] >> 2;
       const double b0 = UU - i2d(ni) * H; // in [0, H)
+      ev.init(st, q, 0.0);
+      if (k == 10) {
 #pragma unroll
-      for (int d = 0; d < 7; ++d) { // left fine loop (LineGridCalc.f90:332-339): i = ni+1-d
-        const int i = ni + 1 - d;
-        if (i >= 2 && i <= NT && ni < 4 * ((i - 2) / 4) + 8) put(d, i - 2, b0 + (double)d * H);
-      }
+        for (int d = 0; d < 7; ++d) { // left fine loop (LineGridCalc.f90:332-339): i = ni+1-d
+          const int i = ni + 1 - d;
+          if (i >= 2 && i <= NT && ni < 4 * ((i - 2) / 4) + 8) put(d, i - 2, b0 + (double)d * H);
+        }
+      } else {
 #pragma unroll
-      for (int d = 0; d < 8; ++d) { // right fine loop (LineGridCalc.f90:485-490): i = ni+2+d
-        const int i = ni + 2 + d;
-        if (i >= 2 && i <= NT && nv9 < (NT - i) / 4 + 2) put(7 + d, i - 2, b0 - (double)(1 + d) * H);
+        for (int d = 0; d < 8; ++d) { // right fine loop (LineGridCalc.f90:485-490): i = ni+2+d
+          const int i = ni + 2 + d;
+          if (i >= 2 && i <= NT && nv9 < (NT - i) / 4 + 2) put(d, i - 2, b0 - (double)(1 + d) * H);
+        }
       }
     } else if (cls == 0) {
-      if (UU > -H9) { // leftLBL label 29: RK(2..5)
-        ev.init(st, q);
+      if (k == 10 && UU > -H9) { // leftLBL label 29: RK(2..5)
+        ev.init(st, q, 0.0);
         put(0, 0, UU - H);
         put(1, 1, (UU - H) - H);
         put(2, 2, (UU + H) - H9);
@@ -844,8 +887,8 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
       }
     } else {
       const double U = UU - DELTA_WV;
-      if (U < H9) { // rightLBL label 69: RK(NT..NT-3)
-        ev.init(st, q);
+      if (k == 11 && U < H9) { // rightLBL label 69: RK(NT..NT-3)
+        ev.init(st, q, 0.0);
         put(0, NT - 2, U);
         put(1, NT - 3, U + H);
         put(2, NT - 4, (U + H) + H);
@@ -876,8 +919,8 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
 // the runs, then a fixed-order group reduction; every lane of the warp calls
 // this the same number of times, and a group whose p lies past the grid sums
 // nothing and stores nothing.
-template <bool F64, int G>
-__device__ void pair_cells(const NearStore<F64> &st, int k, int p, const typename NearStore<F64>::Real *vb,
+template <bool F64>
+__device__ void pair_cells(const NearStore<F64> &st, int k, int p, int G, const typename NearStore<F64>::Real *vb,
                            int cap, typename NearStore<F64>::Real *scr, int lane) {
   using Real = typename NearStore<F64>::Real;
   const int ntk = nt_k(k), np = ntk >> 1, sh = 9 - k;
@@ -949,8 +992,11 @@ __device__ void pair_cells(const NearStore<F64> &st, int k, int p, const typenam
       }
     }
   }
-  const double pa = group_sum<G>(PA.value()), ma = group_sum<G>(MA.value()), la = group_sum<G>(LA.value());
-  const double pb = group_sum<G>(PB.value()), mb = group_sum<G>(MB.value()), lb = group_sum<G>(LB.value());
+  double v[6] = {PA.value(), MA.value(), LA.value(), PB.value(), MB.value(), LB.value()};
+  for (int off = G >> 1; off > 0; off >>= 1)
+#pragma unroll
+    for (int i = 0; i < 6; ++i) v[i] += __shfl_down_sync(0xffffffffu, v[i], off, G);
+  const double pa = v[0], ma = v[1], la = v[2], pb = v[3], mb = v[4], lb = v[5];
   if (valid && lane == 0) {
     const int a = base_k(k) - NT0 + 2 * p - 2; // cell A; cell B follows
     scr[SCR_FINE_P + a] = (Real)pa;
@@ -962,47 +1008,52 @@ __device__ void pair_cells(const NearStore<F64> &st, int k, int p, const typenam
   }
 }
 
-// Site half of the finest pass for the four points i = 4j-2 .. 4j+1 of
+// Site half of the finest passes for the four points i = 4j-2 .. 4j+1 of
 // grid-9 cell j.  They share both outer bounds: the left fine loop ends at
 // (4 floor((i-2)/4) + 8) H = (4j + 4) H and the right fine loop's V bound is
 // (floor((NT-i)/4) + 2) H9 = (5122 - j) H9, so every line of the run
 // [first V < (5122 - j) H9, first UU >= (4j + 4) H) reaches all four points:
-// point i through its left loop (slot floor(UU/H) + 1 - i) when
-// floor(UU/H) >= i - 1, else through its right loop (slot
-// 7 + i - floor(UU/H) - 2).  Then the near lines: RK(2..5) from the near-left
-// lines with D < H9, RK(NT-3..NT) from the near-right lines with U < H9.
+// point i through its left loop (slot floor(UU/H) + 1 - i of pass 10) when
+// floor(UU/H) >= i - 1, else through its right loop (slot i - floor(UU/H) - 2
+// of pass 11).  Pass 10 adds the left loops and, for j = 1, the near-left
+// lines with D < H9 (RK(2..5)) and stores the sums; pass 11 adds the right
+// loops and, for j = 5120, the near-right lines with U < H9 (RK(NT-3..NT)).
 template <bool F64>
-__device__ void quad_points(const NearStore<F64> &st, int j, const typename NearStore<F64>::Real *vb, int cap,
-                            typename NearStore<F64>::Real *scr) {
+__device__ void quad_points(const NearStore<F64> &st, int j, bool left, const typename NearStore<F64>::Real *vb,
+                            int cap, typename NearStore<F64>::Real *scr) {
+  using Real = typename NearStore<F64>::Real;
   const double H9 = h_k(9);
   const int i0 = 4 * j - 2;
+  Real *o = scr + SCR_RK + i0 - 2;
   Acc<F64> a[4];
 #pragma unroll
-  for (int p = 0; p < 4; ++p) a[p].init();
+  for (int p = 0; p < 4; ++p) {
+    a[p].init();
+    if (!left) a[p].add(o[p]);
+  }
   const int q0 = st.bin_v(5122 - j), q1 = st.bin_u(j + 1);
   for (int q = q0; q < q1; ++q) {
     const int ni = st.n11[q];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
       const int i = i0 + p;
-      const int slot = ni >= i - 1 ? ni + 1 - i : 5 + i - ni;
-      a[p].add(vb[(size_t)slot * cap + q]);
+      if (left == (ni >= i - 1)) a[p].add(vb[(size_t)(left ? ni + 1 - i : i - ni - 2) * cap + q]);
     }
   }
-  if (j == 1) { // RK(2..5): near-left lines with D < H9
+  if (left && j == 1) { // RK(2..5): near-left lines with D < H9
     const int qn = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -H9; });
     for (int q = qn; q < st.c0; ++q)
 #pragma unroll
       for (int p = 0; p < 4; ++p) a[p].add(vb[(size_t)p * cap + q]);
   }
-  if (j == NBIN9) { // RK(NT-3..NT): near-right lines with U < H9
+  if (!left && j == NBIN9) { // RK(NT-3..NT): near-right lines with U < H9
     const int qn = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= H9; });
     for (int q = st.c1; q < qn; ++q)
 #pragma unroll
       for (int p = 0; p < 4; ++p) a[p].add(vb[(size_t)(NT - i0 - p) * cap + q]);
   }
 #pragma unroll
-  for (int p = 0; p < 4; ++p) scr[SCR_RK + i0 + p - 2] = (typename NearStore<F64>::Real)a[p].value();
+  for (int p = 0; p < 4; ++p) o[p] = (Real)a[p].value();
 }
 
 __device__ __forceinline__ int block_excl_scan(int v, int &total) {
@@ -1053,9 +1104,10 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   __syncthreads();
   const int64_t a = sb[0], b = sb[3];
   const int cnt = (int)(b - a);
-  // staging area: shared memory, or this block's slice of the global staging buffer
+  // staging area: shared memory at this unit's own size, or this block's
+  // slice of the global staging buffer
   const bool staged_smem = cnt <= p.smem_cap;
-  const int cap = staged_smem ? p.smem_cap : p.gstage_cap;
+  const int cap = staged_smem ? max(32, (cnt + 31) & ~31) : p.gstage_cap;
   unsigned char *base = staged_smem ? fine_smem : (unsigned char *)p.gstage + (size_t)blockIdx.x * p.gstage_bytes;
   NearStore<F64> st;
   st.uu = (double *)base;
@@ -1124,7 +1176,7 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     struct {
       unsigned short u[NBIN9 + 1], v[NBIN9 + 2];
     } first;
-    double red[32][31];
+    double red[32][32];
   } s_tab;
   // grid 0 and RK(1): one thread per near line, block reduction
   {
@@ -1133,16 +1185,16 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
 #pragma unroll
     for (int j = 0; j < 10; ++j) { aP[j].init(); aM[j].init(); aL[j].init(); }
     for (int q = threadIdx.x; q < st.m; q += blockDim.x) grid0_line<F64, CHI>(st, q, aR, aP, aM, aL);
-    double v[31];
-    v[0] = aR.value();
+    Real v[31];
+    v[0] = aR.v;
 #pragma unroll
     for (int j = 0; j < 10; ++j) {
-      v[1 + j] = aP[j].value();
-      v[11 + j] = aM[j].value();
-      v[21 + j] = aL[j].value();
+      v[1 + j] = aP[j].v;
+      v[11 + j] = aM[j].v;
+      v[21 + j] = aL[j].v;
     }
     __shared__ double g0[31];
-    block_reduce_store<31>(v, g0, s_tab.red);
+    block_reduce31<Real>(v, g0, s_tab.red);
     __syncthreads();
     if (threadIdx.x < 31) scr[threadIdx.x] = (Real)g0[threadIdx.x];
   }
@@ -1161,14 +1213,17 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   st.firstU = s_tab.first.u;
   st.firstV = s_tab.first.v;
 
-  // slot buffer: in shared memory behind the staged lines when its rows fit
-  // there (units staged in shared memory only), else this block's global slice
+  // slot buffer: in shared memory behind this unit's staged lines when its
+  // rows fit in the launch's dynamic shared memory, else this block's global
+  // slice
   Real *vb_g = (Real *)p.vbuf + (size_t)blockIdx.x * p.vbuf_stride;
-  Real *vb_s = (Real *)(fine_smem + (size_t)p.smem_cap * (24 + 3 * sizeof(Real) + 4));
-  for (int k = 1; k <= 10; ++k) {
-    const bool vsm = staged_smem && (k <= 9 ? 10 : NSLOT) <= p.vsm_rows;
+  const size_t stage_bytes = (size_t)cap * (24 + 3 * sizeof(Real) + 4);
+  Real *vb_s = (Real *)(fine_smem + stage_bytes);
+  for (int k = 1; k <= 11; ++k) {
+    const int rows = k <= 9 ? 10 : (k == 10 ? 7 : 8);
+    const bool vsm = staged_smem && stage_bytes + (size_t)rows * cap * sizeof(Real) <= p.smem_room;
     Real *vb = vsm ? vb_s : vb_g;
-    const int vcap = vsm ? p.smem_cap : p.vbuf_cap;
+    const int vcap = vsm ? cap : p.vbuf_cap;
     for (int q = threadIdx.x; q < st.m; q += blockDim.x) line_pass<F64, CHI>(st, q, k, vb, vcap);
     __syncthreads();
     if (k <= 9) {
@@ -1182,24 +1237,11 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
         const int want = (int)blockDim.x / np;
         G = want >= 32 ? 32 : want >= 16 ? 16 : want >= 8 ? 8 : want >= 4 ? 4 : want >= 2 ? 2 : 1;
       }
-      if (G == 1) {
-        for (int pp = 1 + threadIdx.x; pp <= np; pp += blockDim.x) pair_cells<F64, 1>(st, k, pp, vb, vcap, scr, 0);
-      } else {
-        const int lane = threadIdx.x & (G - 1), grp = threadIdx.x / G, ngrp = blockDim.x / G;
-        const int rounds = (np + ngrp - 1) / ngrp; // the same for every lane
-        for (int r = 0; r < rounds; ++r) {
-          const int pp = 1 + grp + r * ngrp;
-          switch (G) {
-          case 32: pair_cells<F64, 32>(st, k, pp, vb, vcap, scr, lane); break;
-          case 16: pair_cells<F64, 16>(st, k, pp, vb, vcap, scr, lane); break;
-          case 8: pair_cells<F64, 8>(st, k, pp, vb, vcap, scr, lane); break;
-          case 4: pair_cells<F64, 4>(st, k, pp, vb, vcap, scr, lane); break;
-          default: pair_cells<F64, 2>(st, k, pp, vb, vcap, scr, lane); break;
-          }
-        }
-      }
+      const int lane = threadIdx.x & (G - 1), grp = threadIdx.x / G, ngrp = blockDim.x / G;
+      const int rounds = (np + ngrp - 1) / ngrp; // the same for every lane
+      for (int r = 0; r < rounds; ++r) pair_cells<F64>(st, k, 1 + grp + r * ngrp, G, vb, vcap, scr, lane);
     } else {
-      for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) quad_points<F64>(st, j, vb, vcap, scr);
+      for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) quad_points<F64>(st, j, k == 10, vb, vcap, scr);
     }
     __syncthreads();
   }
@@ -1565,7 +1607,7 @@ constexpr int SMALL_TH = 256;
 
 template <bool F64, int CHI, int TH>
 static cudaError_t fine_launch_th(const FineParams &p, cudaStream_t st) {
-  const size_t smem = fine_smem_bytes(p.smem_cap, F64, p.vsm_rows);
+  const size_t smem = p.smem_room;
   cudaError_t e = cudaFuncSetAttribute(fine_kernel<F64, CHI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   fine_kernel<F64, CHI, TH><<<p.grid, TH, smem, st>>>(p);
@@ -1578,11 +1620,12 @@ static cudaError_t fine_launch(const FineParams &p, cudaStream_t st) {
                                      : fine_launch_th<F64, CHI, fine_threads(F64)>(p, st);
 }
 
-// Shared-memory plan of the fine kernel for `smem_cap` staged lines: the
-// most slot-buffer rows (NSLOT, 10 or 0) that fit beside the staging area,
-// and the resident blocks of the persistent grid.
+// Shared-memory plan of the fine kernel: large blocks (one per SM) take the
+// whole room a block may have and place each unit's slot rows there when
+// they fit; small blocks stage `smem_cap` lines, with slot rows when those
+// fit too.  Also the resident blocks of the persistent grid.
 template <bool F64, int CHI, int TH>
-static cudaError_t fine_occupancy_th(int smem_cap, int *rows, int *blocks) {
+static cudaError_t fine_occupancy_th(int smem_cap, size_t *smem_room, int *blocks) {
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI, TH>);
   if (e != cudaSuccess) return e;
@@ -1591,10 +1634,10 @@ static cudaError_t fine_occupancy_th(int smem_cap, int *rows, int *blocks) {
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
   const size_t room = (size_t)optin - fa.sharedSizeBytes;
-  *rows = 0;
-  for (int r : {NSLOT, 10})
-    if (fine_smem_bytes(smem_cap, F64, r) <= room) { *rows = r; break; }
-  const size_t smem = fine_smem_bytes(smem_cap, F64, *rows);
+  size_t smem = room;
+  if (TH == SMALL_TH)
+    smem = fine_smem_bytes(smem_cap, F64, fine_smem_bytes(smem_cap, F64, NSLOT) <= room ? NSLOT : 0);
+  *smem_room = smem;
   if ((e = cudaFuncSetAttribute(fine_kernel<F64, CHI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
     return e;
   int per_sm = 0;
@@ -1626,9 +1669,9 @@ static cudaError_t fine_stage_limit(int threads, int *lines) {
 }
 
 template <bool F64, int CHI>
-static cudaError_t fine_occupancy(int threads, int smem_cap, int *rows, int *blocks) {
-  return threads == SMALL_TH ? fine_occupancy_th<F64, CHI, SMALL_TH>(smem_cap, rows, blocks)
-                             : fine_occupancy_th<F64, CHI, fine_threads(F64)>(smem_cap, rows, blocks);
+static cudaError_t fine_occupancy(int threads, int smem_cap, size_t *room, int *blocks) {
+  return threads == SMALL_TH ? fine_occupancy_th<F64, CHI, SMALL_TH>(smem_cap, room, blocks)
+                             : fine_occupancy_th<F64, CHI, fine_threads(F64)>(smem_cap, room, blocks);
 }
 
 template <bool F64>
@@ -1642,18 +1685,18 @@ static cudaError_t fine_dispatch(const FineParams &p, int chi, cudaStream_t st) 
 }
 
 template <bool F64>
-static cudaError_t fine_occ_dispatch(int chi, int threads, int smem_cap, int *rows, int *blocks) {
+static cudaError_t fine_occ_dispatch(int chi, int threads, int smem_cap, size_t *room, int *blocks) {
   switch (chi) {
-  case CHI_TONKOV: return fine_occupancy<F64, CHI_TONKOV>(threads, smem_cap, rows, blocks);
-  case CHI_POLLACK: return fine_occupancy<F64, CHI_POLLACK>(threads, smem_cap, rows, blocks);
-  case CHI_PERRIN: return fine_occupancy<F64, CHI_PERRIN>(threads, smem_cap, rows, blocks);
-  default: return fine_occupancy<F64, CHI_NONE>(threads, smem_cap, rows, blocks);
+  case CHI_TONKOV: return fine_occupancy<F64, CHI_TONKOV>(threads, smem_cap, room, blocks);
+  case CHI_POLLACK: return fine_occupancy<F64, CHI_POLLACK>(threads, smem_cap, room, blocks);
+  case CHI_PERRIN: return fine_occupancy<F64, CHI_PERRIN>(threads, smem_cap, room, blocks);
+  default: return fine_occupancy<F64, CHI_NONE>(threads, smem_cap, room, blocks);
   }
 }
 
-size_t fine_smem_bytes(int cap, bool f64, int vsm_rows) {
+size_t fine_smem_bytes(int cap, bool f64, int rows) {
   const size_t r = f64 ? 8 : 4;
-  return (size_t)cap * (24 + 3 * r + 4 + (size_t)vsm_rows * r);
+  return (size_t)cap * (24 + 3 * r + 4 + (size_t)rows * r);
 }
 size_t fine_vbuf_elems(int cap) { return (size_t)NSLOT * cap; }
 
@@ -1671,9 +1714,9 @@ cudaError_t fine_smem_lines(int precision, int chi, int threads, int *lines) {
   }
 }
 
-cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, int *vsm_rows, int *blocks) {
-  return precision == 0 ? fine_occ_dispatch<true>(chi, threads, smem_cap, vsm_rows, blocks)
-                        : fine_occ_dispatch<false>(chi, threads, smem_cap, vsm_rows, blocks);
+cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, size_t *smem_room, int *blocks) {
+  return precision == 0 ? fine_occ_dispatch<true>(chi, threads, smem_cap, smem_room, blocks)
+                        : fine_occ_dispatch<false>(chi, threads, smem_cap, smem_room, blocks);
 }
 
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st) {

@@ -67,9 +67,9 @@ struct FarParams {
   double *out;                   // [Lc][C][NFAR]
 };
 
-// Rows of the fine kernel's slot buffer (values per staged line; the
-// finest-point pass uses 15).
-constexpr int NSLOT = 15;
+// Rows of the fine kernel's slot buffer (values per staged line: ten on
+// grids 1..9, seven and eight in the two finest-point passes).
+constexpr int NSLOT = 10;
 
 struct FineParams {
   const double *snu;
@@ -96,7 +96,8 @@ struct FineParams {
   size_t vbuf_stride;            // elements per block
   int vbuf_cap;                  // lines per slot row in vbuf
   int grid;                      // persistent blocks
-  int vsm_rows;                  // slot-buffer rows held in shared memory (0, 10 or NSLOT)
+  size_t smem_room;              // dynamic shared memory of the launch (bytes): a unit keeps its
+                                 // slot rows there when they fit beside its staged lines
   int coop_k;                    // grids 1..coop_k: lane groups per cell pair in the site half
   int block_threads;             // threads per block (fine_block_threads)
 };
@@ -194,9 +195,9 @@ cudaError_t launch_sort(const SortParams &p, cudaStream_t st);
 cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t st);
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st);
 cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st);
-// dynamic shared memory of the fine kernel: `cap` staged lines and
-// `vsm_rows` slot-buffer rows of `cap` values
-size_t fine_smem_bytes(int cap, bool f64, int vsm_rows = 0);
+// shared memory of `cap` staged lines and `rows` slot-buffer rows of `cap`
+// values
+size_t fine_smem_bytes(int cap, bool f64, int rows = 0);
 size_t fine_vbuf_elems(int cap);
 // block size of the fine kernel for a batch whose units have at most
 // `max_near` near lines (small blocks below `small_below` lines)
@@ -204,8 +205,10 @@ int fine_block_threads(int precision, int max_near, int small_below);
 // most near lines a block of `threads` stages in shared memory (the opt-in
 // limit minus the kernel's static shared memory)
 cudaError_t fine_smem_lines(int precision, int chi, int threads, int *lines);
-// slot-buffer rows that fit in shared memory and the persistent grid size
-cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, int *vsm_rows, int *blocks);
+// dynamic shared memory of the launch and the persistent grid size: the whole
+// per-block room for the large blocks, `smem_cap` lines (with slot rows when
+// they fit) for the small ones
+cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, size_t *smem_room, int *blocks);
 cudaError_t fma_peak(bool f64, double *flops_per_s);
 cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st);
 cudaError_t launch_count(const CountParams &p, cudaStream_t st);

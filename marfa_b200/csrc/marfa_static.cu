@@ -362,7 +362,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   fn.queue = &d_small->queue;
   fn.order = nullptr;
   fn.grid = 1;
-  fn.vsm_rows = 0;
+  fn.smem_room = fine_smem_bytes(fn.smem_cap, f64);
   fn.coop_k = 5;
   fn.vbuf = base + OFF_VB;
   fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
