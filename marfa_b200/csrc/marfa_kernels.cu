@@ -627,9 +627,8 @@ __device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Lane
 }
 
 // ----------------------------------------------------------- fine grids
-// Grids 1..9 and the direct finest points are computed in eleven passes (one
-// per grid, then the finest points of the left fine loops and of the right
-// fine loops).  Each pass has two halves:
+// Grids 1..9 and the direct finest points are computed in ten passes (one
+// per grid, then the finest points).  Each pass has two halves:
 //   line half  one thread per near line evaluates every cell of the pass's
 //              grid that the line's walk visits (centerLBL, and the fine
 //              parts of leftLBL / rightLBL).  The line's Kuntz coefficients
@@ -857,28 +856,23 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
       }
     }
   } else {
-    // the finest points in two passes: k = 10 the left fine loops and the
-    // near-left lines, k = 11 the right fine loops and the near-right lines
     const double H = HSTEP, H9 = h_k(9);
     if (cls == 1) {
       const int ni = st.n11[q], nv9 = st.nv11[q] >> 2;
       const double b0 = UU - i2d(ni) * H; // in [0, H)
       ev.init(st, q, 0.0);
-      if (k == 10) {
 #pragma unroll
-        for (int d = 0; d < 7; ++d) { // left fine loop (LineGridCalc.f90:332-339): i = ni+1-d
-          const int i = ni + 1 - d;
-          if (i >= 2 && i <= NT && ni < 4 * ((i - 2) / 4) + 8) put(d, i - 2, b0 + (double)d * H);
-        }
-      } else {
+      for (int d = 0; d < 7; ++d) { // left fine loop (LineGridCalc.f90:332-339): i = ni+1-d
+        const int i = ni + 1 - d;
+        if (i >= 2 && i <= NT && ni < 4 * ((i - 2) / 4) + 8) put(d, i - 2, b0 + (double)d * H);
+      }
 #pragma unroll
-        for (int d = 0; d < 8; ++d) { // right fine loop (LineGridCalc.f90:485-490): i = ni+2+d
-          const int i = ni + 2 + d;
-          if (i >= 2 && i <= NT && nv9 < (NT - i) / 4 + 2) put(d, i - 2, b0 - (double)(1 + d) * H);
-        }
+      for (int d = 0; d < 8; ++d) { // right fine loop (LineGridCalc.f90:485-490): i = ni+2+d
+        const int i = ni + 2 + d;
+        if (i >= 2 && i <= NT && nv9 < (NT - i) / 4 + 2) put(7 + d, i - 2, b0 - (double)(1 + d) * H);
       }
     } else if (cls == 0) {
-      if (k == 10 && UU > -H9) { // leftLBL label 29: RK(2..5)
+      if (UU > -H9) { // leftLBL label 29: RK(2..5)
         ev.init(st, q, 0.0);
         put(0, 0, UU - H);
         put(1, 1, (UU - H) - H);
@@ -887,7 +881,7 @@ __device__ void line_pass(const NearStore<F64> &st, int q, int k, typename NearS
       }
     } else {
       const double U = UU - DELTA_WV;
-      if (k == 11 && U < H9) { // rightLBL label 69: RK(NT..NT-3)
+      if (U < H9) { // rightLBL label 69: RK(NT..NT-3)
         ev.init(st, q, 0.0);
         put(0, NT - 2, U);
         put(1, NT - 3, U + H);
@@ -1008,45 +1002,43 @@ __device__ void pair_cells(const NearStore<F64> &st, int k, int p, int G, const 
   }
 }
 
-// Site half of the finest passes for the four points i = 4j-2 .. 4j+1 of
+// Site half of the finest pass for the four points i = 4j-2 .. 4j+1 of
 // grid-9 cell j.  They share both outer bounds: the left fine loop ends at
 // (4 floor((i-2)/4) + 8) H = (4j + 4) H and the right fine loop's V bound is
 // (floor((NT-i)/4) + 2) H9 = (5122 - j) H9, so every line of the run
 // [first V < (5122 - j) H9, first UU >= (4j + 4) H) reaches all four points:
-// point i through its left loop (slot floor(UU/H) + 1 - i of pass 10) when
-// floor(UU/H) >= i - 1, else through its right loop (slot i - floor(UU/H) - 2
-// of pass 11).  Pass 10 adds the left loops and, for j = 1, the near-left
-// lines with D < H9 (RK(2..5)) and stores the sums; pass 11 adds the right
-// loops and, for j = 5120, the near-right lines with U < H9 (RK(NT-3..NT)).
+// point i through its left loop (slot floor(UU/H) + 1 - i) when
+// floor(UU/H) >= i - 1, else through its right loop (slot
+// 7 + i - floor(UU/H) - 2).  Then the near lines: RK(2..5) from the
+// near-left lines with D < H9, RK(NT-3..NT) from the near-right lines with
+// U < H9.
 template <bool F64>
-__device__ void quad_points(const NearStore<F64> &st, int j, bool left, const typename NearStore<F64>::Real *vb,
-                            int cap, typename NearStore<F64>::Real *scr) {
+__device__ void quad_points(const NearStore<F64> &st, int j, const typename NearStore<F64>::Real *vb, int cap,
+                            typename NearStore<F64>::Real *scr) {
   using Real = typename NearStore<F64>::Real;
   const double H9 = h_k(9);
   const int i0 = 4 * j - 2;
   Real *o = scr + SCR_RK + i0 - 2;
   Acc<F64> a[4];
 #pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    a[p].init();
-    if (!left) a[p].add(o[p]);
-  }
+  for (int p = 0; p < 4; ++p) a[p].init();
   const int q0 = st.bin_v(5122 - j), q1 = st.bin_u(j + 1);
   for (int q = q0; q < q1; ++q) {
     const int ni = st.n11[q];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
       const int i = i0 + p;
-      if (left == (ni >= i - 1)) a[p].add(vb[(size_t)(left ? ni + 1 - i : i - ni - 2) * cap + q]);
+      const int slot = ni >= i - 1 ? ni + 1 - i : 5 + i - ni;
+      a[p].add(vb[(size_t)slot * cap + q]);
     }
   }
-  if (left && j == 1) { // RK(2..5): near-left lines with D < H9
+  if (j == 1) { // RK(2..5): near-left lines with D < H9
     const int qn = gallop_lb(0, st.c0, [&](int q) { return st.uu[q] > -H9; });
     for (int q = qn; q < st.c0; ++q)
 #pragma unroll
       for (int p = 0; p < 4; ++p) a[p].add(vb[(size_t)p * cap + q]);
   }
-  if (!left && j == NBIN9) { // RK(NT-3..NT): near-right lines with U < H9
+  if (j == NBIN9) { // RK(NT-3..NT): near-right lines with U < H9
     const int qn = gallop_lb(st.c1, st.m, [&](int q) { return (st.uu[q] - DELTA_WV) >= H9; });
     for (int q = st.c1; q < qn; ++q)
 #pragma unroll
@@ -1219,8 +1211,8 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
   Real *vb_g = (Real *)p.vbuf + (size_t)blockIdx.x * p.vbuf_stride;
   const size_t stage_bytes = (size_t)cap * (24 + 3 * sizeof(Real) + 4);
   Real *vb_s = (Real *)(fine_smem + stage_bytes);
-  for (int k = 1; k <= 11; ++k) {
-    const int rows = k <= 9 ? 10 : (k == 10 ? 7 : 8);
+  for (int k = 1; k <= 10; ++k) {
+    const int rows = k <= 9 ? 10 : NSLOT;
     const bool vsm = staged_smem && stage_bytes + (size_t)rows * cap * sizeof(Real) <= p.smem_room;
     Real *vb = vsm ? vb_s : vb_g;
     const int vcap = vsm ? cap : p.vbuf_cap;
@@ -1241,7 +1233,7 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
       const int rounds = (np + ngrp - 1) / ngrp; // the same for every lane
       for (int r = 0; r < rounds; ++r) pair_cells<F64>(st, k, 1 + grp + r * ngrp, G, vb, vcap, scr, lane);
     } else {
-      for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) quad_points<F64>(st, j, k == 10, vb, vcap, scr);
+      for (int j = 1 + threadIdx.x; j <= NBIN9; j += blockDim.x) quad_points<F64>(st, j, vb, vcap, scr);
     }
     __syncthreads();
   }

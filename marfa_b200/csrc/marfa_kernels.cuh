@@ -68,8 +68,8 @@ struct FarParams {
 };
 
 // Rows of the fine kernel's slot buffer (values per staged line: ten on
-// grids 1..9, seven and eight in the two finest-point passes).
-constexpr int NSLOT = 10;
+// grids 1..9, fifteen in the finest-point pass).
+constexpr int NSLOT = 15;
 
 struct FineParams {
   const double *snu;
