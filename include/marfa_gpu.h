@@ -253,11 +253,6 @@ int marfa_compute_record_static(const marfa_line_record *lines, int64_t n_lines,
                                 double temperature, double density, int isub, float *record,
                                 void *stream, char *msg, size_t msg_len);
 
-/* Measured FP32 and FP64 FMA throughput of `device` (FLOP/s, FMA = 2):
- * the denominators of the shape kernels' roofline, which run on the
- * non-tensor FP32 / FP64 pipes. */
-int marfa_measure_fma_peak(int device, double *fp32_flops, double *fp64_flops);
-
 #ifdef __cplusplus
 }
 #endif

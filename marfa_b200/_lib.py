@@ -21,7 +21,7 @@ EXPORTS = (
     "marfa_ctx_create", "marfa_ctx_destroy", "marfa_last_error", "marfa_num_subintervals",
     "marfa_record_number", "marfa_compute", "marfa_compute_batched", "marfa_compute_device",
     "marfa_synchronize", "marfa_eval_count", "marfa_debug_accumulators", "marfa_last_timings",
-    "marfa_plan_windows", "marfa_measure_fma_peak", "marfa_compute_record_static",
+    "marfa_plan_windows", "marfa_compute_record_static",
     "marfa_ctx_set_line_params", "marfa_vjp", "marfa_graph_create", "marfa_graph_launch",
     "marfa_graph_destroy", "marfa_autotune",
 )
@@ -73,7 +73,6 @@ def load():
         "marfa_debug_accumulators": (I, [P, ctypes.POINTER(MarfaRun), P, P, P, I, I, I, P]),
         "marfa_last_timings": (I, [P, P]),
         "marfa_plan_windows": (I, [P, I64, D, D, D, P, P]),
-        "marfa_measure_fma_peak": (I, [I, P, P]),
         "marfa_compute_record_static": (I, [P, I64, P, I, I, ctypes.POINTER(MarfaRun), D, D, D, I, P,
                                             P, ctypes.c_char_p, ctypes.c_size_t]),
         "marfa_ctx_set_line_params": (I, [P, P, P]),

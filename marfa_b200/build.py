@@ -19,6 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libmarfa_gpu.so"
+PROBE = PKG / "libmarfa_probe.so"   # FMA throughput probe of the benchmark
 CLI = PKG / "marfa"
 SOURCES = ["marfa_kernels.cu", "marfa_adjoint.cu", "marfa_api.cu", "marfa_static.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -49,7 +50,7 @@ def stale() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
-    if not CLI.exists():
+    if not CLI.exists() or not PROBE.exists():
         return True
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + \
         list(CSRC.glob("*.cpp")) + \
@@ -69,6 +70,12 @@ def build(force: bool = False, extra=()) -> Path:
     if r.returncode:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    # the benchmark's FMA throughput probe (a library of its own, not part of
+    # the line-by-line interface)
+    cmd = [nvcc(), *flags(), "-shared", "-cudart", "static", str(CSRC / "marfa_probe.cu"), "-o", str(PROBE)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode:
+        raise RuntimeError(f"probe build failed:\n{r.stdout}\n{r.stderr}")
     # the `marfa` command (host driver over the C ABI)
     cmd = [nvcc(), "-O2", "-std=c++17", "-I", str(ROOT / "include"), str(CSRC / "marfa_cli.cpp"),
            "-o", str(CLI), "-L", str(PKG), "-lmarfa_gpu", "-Xlinker", "-rpath=$ORIGIN"]

@@ -208,11 +208,21 @@ struct Staging {
         (e = cudaEventCreateWithFlags(&ctx->pinned_ev[slot], cudaEventDisableTiming)))
       return e;
     if (bytes > ctx->pinned_cap[slot]) {
-      if (ctx->pinned[slot]) cudaFreeHost(ctx->pinned[slot]);
-      ctx->pinned[slot] = nullptr;
-      ctx->pinned_cap[slot] = 0;
-      if ((e = cudaMallocHost(&ctx->pinned[slot], bytes))) return e;
-      ctx->pinned_cap[slot] = bytes;
+      // pinned allocation synchronizes the device: grow every slot of the
+      // ring at once (with headroom), so that later calls never allocate
+      const size_t cap = bytes + bytes / 2 + 4096;
+      for (int s = 0; s < marfa_ctx::NPIN; ++s) {
+        if (ctx->pinned_pending[s]) {
+          if ((e = cudaEventSynchronize(ctx->pinned_ev[s]))) return e;
+          ctx->pinned_pending[s] = false;
+        }
+        if (ctx->pinned_cap[s] >= cap) continue;
+        if (ctx->pinned[s]) cudaFreeHost(ctx->pinned[s]);
+        ctx->pinned[s] = nullptr;
+        ctx->pinned_cap[s] = 0;
+        if ((e = cudaMallocHost(&ctx->pinned[s], cap))) return e;
+        ctx->pinned_cap[s] = cap;
+      }
     }
     off = 0;
     return e;
@@ -1519,14 +1529,6 @@ int marfa_debug_accumulators(marfa_ctx *ctx, const marfa_run *run, const double 
   } catch (...) {
     return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
   }
-}
-
-int marfa_measure_fma_peak(int device, double *fp32_flops, double *fp64_flops) {
-  if (!fp32_flops || !fp64_flops) return MARFA_E_ARG;
-  if (cudaSetDevice(device) != cudaSuccess) return MARFA_E_NODEVICE;
-  if (fma_peak(false, fp32_flops) != cudaSuccess) return MARFA_E_CUDA;
-  if (fma_peak(true, fp64_flops) != cudaSuccess) return MARFA_E_CUDA;
-  return MARFA_OK;
 }
 
 int marfa_last_timings(marfa_ctx *ctx, double *times) {

@@ -1302,60 +1302,55 @@ __global__ void __launch_bounds__(256) cascade_kernel(CascadeParams p) {
   const int l = u / p.n_sub, sub = u - l * p.n_sub;
   const Real *scr = (const Real *)p.scratch + (size_t)ub * SCR_STRIDE;
   const double inv = p.inv_sscale;
-  __shared__ double bufA[512 * 3];
-  __shared__ double bufB[512 * 3];
   __shared__ float outb[2048];
-  __shared__ double rk1;
-  if (threadIdx.x < 32) { // grid-0 cell J: far-line sums + near part
-    double f[4];
-    far_cell_sums(p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
-    if (threadIdx.x == 0) {
-      bufA[0] = (f[0] + (double)scr[1 + J - 1]) * inv;
-      bufA[1] = (f[1] + (double)scr[11 + J - 1]) * inv;
-      bufA[2] = (f[2] + (double)scr[21 + J - 1]) * inv;
-      rk1 = (f[3] + (double)scr[0]) * inv;
+  // grid-0 cell J: far-line sums (every warp reduces them itself, in the same
+  // order) plus the near part
+  double f[4];
+  far_cell_sums(p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
+  double cP = (f[0] + (double)scr[1 + J - 1]) * inv;
+  double cM = (f[1] + (double)scr[11 + J - 1]) * inv;
+  double cL = (f[2] + (double)scr[21 + J - 1]) * inv;
+  // thread t walks its grid-8 cell's chain of ancestors, grids 1 .. 8, then
+  // the cell's two grid-9 children (the ancestors of a warp's cells coincide
+  // on the coarse grids: those loads are broadcasts; every address is known
+  // up front, so the unrolled walk issues the loads together)
+  const int t = threadIdx.x;
+  auto refine = [&](int k, int c, double &P, double &M, double &L) {
+    const int idx = base_k(k) - NT0 + (J - 1) * (1 << k) + c;
+    const double oP = (double)scr[SCR_FINE_P + idx] * inv;
+    const double oM = (double)scr[SCR_FINE_M + idx] * inv;
+    const double oL = (double)scr[SCR_FINE_L + idx] * inv;
+    if ((c & 1) == 0) { // finer cell 2J-1 (Grids.f90:86-93)
+      P = oP + cP; M = oM + quarter(cP, cM, cL); L = oL + cM;
+    } else {            // finer cell 2J (Grids.f90:94-101)
+      P = oP + cM; M = oM + quarter(cL, cM, cP); L = oL + cL;
     }
-  }
-  __syncthreads();
-  double *prev = bufA, *cur = bufB;
-  for (int k = 1; k <= 9; ++k) {
-    const int ncell = 1 << k;
-    const int cb = base_k(k) - NT0 + (J - 1) * ncell;
-    for (int t = threadIdx.x; t < ncell; t += blockDim.x) {
-      const int pt = t >> 1;
-      const double cP = prev[3 * pt], cM = prev[3 * pt + 1], cL = prev[3 * pt + 2];
-      double P = (double)scr[SCR_FINE_P + cb + t] * inv;
-      double M = (double)scr[SCR_FINE_M + cb + t] * inv;
-      double L = (double)scr[SCR_FINE_L + cb + t] * inv;
-      if ((t & 1) == 0) { // finer cell 2J-1
-        P += cP; M += quarter(cP, cM, cL); L += cM;
-      } else {            // finer cell 2J
-        P += cM; M += quarter(cL, cM, cP); L += cL;
-      }
-      cur[3 * t] = P;
-      cur[3 * t + 1] = M;
-      cur[3 * t + 2] = L;
-    }
-    __syncthreads();
-    double *tmp = prev; prev = cur; cur = tmp;
+  };
+#pragma unroll
+  for (int k = 1; k <= 8; ++k) {
+    double P, M, L;
+    refine(k, t >> (8 - k), P, M, L);
+    cP = P; cM = M; cL = L;
   }
   // grid 9 -> finest points RK(4j-2 .. 4j+1), j = grid-9 cell (Grids.f90:121-138)
   const double dens = p.target == 1 ? p.lv[l].density : 1.0;
   const size_t rec = ((size_t)(p.level_out0 + l) * p.n_sub + sub) * NT;
-  for (int t = threadIdx.x; t < 512; t += blockDim.x) {
-    const double cP = prev[3 * t], cM = prev[3 * t + 1], cL = prev[3 * t + 2];
-    const int j = (J - 1) * 512 + t + 1;
-    const double v[4] = {quarter(cP, cM, cL), cM, quarter(cL, cM, cP), cL};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    double P, M, L;
+    refine(9, 2 * t + h, P, M, L);
+    const int j = (J - 1) * 512 + 2 * t + h + 1;
+    const double v[4] = {quarter(P, M, L), M, quarter(L, M, P), L};
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int i = 4 * j - 2 + q; // RK index, 1-based
       const double x = ((double)scr[SCR_RK + i - 2] * inv + v[q]) * dens;
-      outb[4 * t + q] = (float)x;
+      outb[8 * t + 4 * h + q] = (float)x;
       if (p.out64) p.out64[rec + i - 1] = x;
     }
   }
-  if (J == 1 && threadIdx.x == 0) {
-    const double x = rk1 * dens;
+  if (J == 1 && t == 0) {
+    const double x = (f[3] + (double)scr[0]) * inv * dens;
     p.out[rec] = (float)x;
     if (p.out64) p.out64[rec] = x;
   }
@@ -1366,9 +1361,9 @@ __global__ void __launch_bounds__(256) cascade_kernel(CascadeParams p) {
   if ((int)threadIdx.x < head) dst[threadIdx.x] = outb[threadIdx.x];
   const int nvec = (2048 - head) >> 2;
   float4 *dv = (float4 *)(dst + head);
-  for (int t = threadIdx.x; t < nvec; t += blockDim.x) {
-    const int o = head + 4 * t;
-    dv[t] = make_float4(outb[o], outb[o + 1], outb[o + 2], outb[o + 3]);
+  for (int t2 = threadIdx.x; t2 < nvec; t2 += blockDim.x) {
+    const int o = head + 4 * t2;
+    dv[t2] = make_float4(outb[o], outb[o + 1], outb[o + 2], outb[o + 3]);
   }
   const int tail0 = head + 4 * nvec;
   if ((int)threadIdx.x < 2048 - tail0) dst[tail0 + threadIdx.x] = outb[tail0 + threadIdx.x];
@@ -1497,54 +1492,6 @@ __global__ void __launch_bounds__(256) count_kernel(CountParams p) {
     p.out[2 * (size_t)item] = t;
     p.out[2 * (size_t)item + 1] = tf;
   }
-}
-
-// ------------------------------------------------------- pipe peak probes
-// Chains of independent FMAs: the measured FP32 / FP64 FMA throughput of this
-// GPU, used as the roofline denominator of the (non-tensor) shape kernels.
-template <typename T>
-__global__ void __launch_bounds__(256) fma_peak_kernel(T *sink, int iters, T a, T b) {
-  T x[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) x[j] = (T)(threadIdx.x + j);
-  for (int i = 0; i < iters; ++i) {
-#pragma unroll
-    for (int j = 0; j < 8; ++j) x[j] = x[j] * a + b;
-  }
-  T s = 0;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) s += x[j];
-  if (s == (T)-1.2345) sink[threadIdx.x] = s; // keeps the chains alive
-}
-
-cudaError_t fma_peak(bool f64, double *flops_per_s) {
-  int dev = 0, nsm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  void *sink = nullptr;
-  cudaError_t e = cudaMalloc(&sink, 4096);
-  if (e != cudaSuccess) return e;
-  const int blocks = nsm * 8, iters = f64 ? 4096 : 16384;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  float best = 1e30f;
-  for (int rep = 0; rep < 4; ++rep) {
-    cudaEventRecord(e0);
-    if (f64) fma_peak_kernel<double><<<blocks, 256>>>((double *)sink, iters, 0.999999, 1e-7);
-    else fma_peak_kernel<float><<<blocks, 256>>>((float *)sink, iters, 0.9999f, 1e-7f);
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (rep > 0) best = ms < best ? ms : best;
-  }
-  e = cudaGetLastError();
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaFree(sink);
-  *flops_per_s = 2.0 * 8.0 * (double)iters * blocks * 256 / (best * 1e-3);
-  return e;
 }
 
 // --------------------------------------------------------------- launchers

@@ -209,7 +209,6 @@ cudaError_t fine_smem_lines(int precision, int chi, int threads, int *lines);
 // per-block room for the large blocks, `smem_cap` lines (with slot rows when
 // they fit) for the small ones
 cudaError_t fine_plan(int precision, int chi, int threads, int smem_cap, size_t *smem_room, int *blocks);
-cudaError_t fma_peak(bool f64, double *flops_per_s);
 cudaError_t launch_cascade(const CascadeParams &p, int precision, cudaStream_t st);
 cudaError_t launch_count(const CountParams &p, cudaStream_t st);
 
