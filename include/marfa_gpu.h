@@ -232,19 +232,24 @@ int marfa_last_timings(marfa_ctx *ctx, double *times);
  * cudaMalloc's implicit device synchronisation.  All device working storage
  * is one static array of MARFA_STATIC_SCRATCH_BYTES inside the library, held
  * by every GPU that loads the library until the process exits.
- *   lines, n_lines: all line records (sorted, ending beyond the last window);
- *   only the window of subinterval `isub` (at most
+ *   lines, n_lines: all line records, sorted by centre (as the reference's
+ *   databases are) and ending beyond the last window; the window of
+ *   subinterval `isub` is found by binary searches, and only its records are
+ *   checked for order (MARFA_E_UNSORTED) and copied to the device (at most
  *   MARFA_STATIC_MAX_WINDOW_LINES lines, of which at most
  *   MARFA_STATIC_MAX_NEAR_LINES within 1 cm-1 of the subinterval when they do
  *   not fit on chip) is copied to the device; larger inputs return
  *   MARFA_E_CAPACITY.
  *   tips: [n_iso][n_temp] (at most 131,072 values); pressure, temperature,
  *   density: the level; record: 20481 floats, host or device memory.
- *   stream: cudaStream_t or NULL; the call waits for its work to finish.
+ *   stream: cudaStream_t or NULL; the call waits for its work to finish
+ *   (it synchronises the stream and copies from pageable host memory, so it
+ *   cannot be called on a stream that is being captured into a graph).
  *   msg (optional): receives a text description of a failure.
- * The first call on each device looks up the array's device address and
- * should come before any stream capture.  Every call on a device reuses the
- * same array: calls that overlap on the GPU race. */
+ * The first call on each device looks up the array's device address.  Every
+ * call on a device reuses the same array: calls that overlap on the GPU
+ * (from two host threads, or on two streams) race, so callers serialise
+ * them. */
 #define MARFA_STATIC_MAX_WINDOW_LINES 65536
 #define MARFA_STATIC_MAX_NEAR_LINES 8192
 #define MARFA_STATIC_SCRATCH_BYTES (12u * 1024u * 1024u)

@@ -17,6 +17,7 @@
 
 #include "marfa_gpu.h"
 #include "marfa_kernels.cuh"
+#include "marfa_windows.h"
 
 using namespace marfa;
 
@@ -268,48 +269,11 @@ struct Plan {
   int max_chunks = 0;             // most chunks of one subinterval
 };
 
-// Windows of all subintervals; returns 0 or MARFA_E_DB with `bad` = the
-// subinterval whose scan ran off the end (-1: before the starting line).
+// Windows of all subintervals (marfa_windows.h).
 int plan_windows(const double *nu, int64_t n, double start_wv, double end_wv, double cut,
                  std::vector<double> &ss, std::vector<double> &se, std::vector<int64_t> &lo,
                  std::vector<int64_t> &hi, int &bad) {
-  const int nsub = marfa_num_subintervals(start_wv, end_wv);
-  bad = -1;
-  // determineStartingSpectralLine (main.f90:196-248): the first record with
-  // nu > start - cutoff.  The line list is sorted, so the reference's linear
-  // scans are binary searches here, with the same results.
-  int64_t start_idx = 0;
-  double start_line = nu[0];
-  if (start_wv > cut) {
-    const double ext = start_wv - cut;
-    start_idx = std::upper_bound(nu, nu + n, ext) - nu;
-    if (start_idx >= n) return MARFA_E_DB;
-    start_line = nu[start_idx];
-  }
-  // SUBINTERVALS_LOOP with the lblScheme window recurrence: the scan from
-  // line_idx stops at the first nu >= start + 10 + cutoff; the next window
-  // starts at the last scanned line with nu <= capWV (or stays)
-  int64_t line_idx = start_idx;
-  double s = start_wv;
-  for (int isub = 0; isub < nsub; ++isub) {
-    const double ext_end = s + DELTA_WV + cut;
-    double cap = (s - cut) + DELTA_WV;
-    if (cap <= start_line) cap = start_line;
-    const int64_t I = std::lower_bound(nu + line_idx, nu + n, ext_end) - nu;
-    if (I >= n) {
-      bad = isub;
-      return MARFA_E_DB;
-    }
-    const int64_t last = (std::upper_bound(nu + line_idx, nu + I, cap) - nu) - 1;
-    const int64_t next = last >= line_idx ? last : line_idx;
-    ss.push_back(s);
-    se.push_back(s + DELTA_WV);
-    lo.push_back(line_idx);
-    hi.push_back(I);
-    line_idx = next;
-    s = s + DELTA_WV;
-  }
-  return MARFA_OK;
+  return plan_windows_of(nu, n, start_wv, marfa_num_subintervals(start_wv, end_wv), cut, ss, se, lo, hi, bad);
 }
 
 int make_plan(marfa_ctx *ctx, const marfa_run *run, Plan &pl) {

@@ -29,6 +29,7 @@
 
 #include "marfa_gpu.h"
 #include "marfa_kernels.cuh"
+#include "marfa_windows.h"
 
 using namespace marfa;
 
@@ -96,16 +97,25 @@ int scratch_address(int dev, unsigned char **out, char *msg, size_t len) {
   return MARFA_OK;
 }
 
-double rec_nu(const marfa_line_record *r, int64_t i) { return r[i].nu; }
+double rec_nu(const marfa_line_record *r, int64_t i) { return *RecordNu{r + i}; }
 
-// isotopologue index from the copied jointMolIso field, in place
-__global__ void iso_from_joint_kernel(int *v, int64_t n) {
+// The window's packed 36-byte records (copied in one piece) split into the
+// field arrays of the kernels, with the isotopologue index jointMolIso / 100
+// (LBL.f90:64-65).  Records start 4-byte aligned: every field is read as
+// 32-bit words.
+__global__ void split_records_kernel(const unsigned *raw, int64_t n, double *nu, float *f32, int *iso, int64_t stride) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) v[i] = v[i] / 100;
+  if (i >= n) return;
+  const unsigned *w = raw + 9 * i; // 36 bytes = 9 words
+  nu[i] = __hiloint2double((int)w[1], (int)w[0]);
+  for (int f = 0; f < 5; ++f) f32[f * stride + i] = __uint_as_float(w[2 + f]); // S, gair, gself, E, nair
+  iso[i] = (int)w[7] / 100;
+  f32[5 * stride + i] = __uint_as_float(w[8]); // delta_air
 }
 
-cudaError_t iso_from_joint(int *v, int64_t n, cudaStream_t st) {
-  iso_from_joint_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, n);
+cudaError_t split_records(const void *raw, int64_t n, double *nu, float *f32, int *iso, int64_t stride,
+                          cudaStream_t st) {
+  split_records_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const unsigned *)raw, n, nu, f32, iso, stride);
   return cudaGetLastError();
 }
 
@@ -126,41 +136,23 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   if (run->mol_code < 1 || run->mol_code > 12) return fail(msg, msg_len, 8, "unsupported molecule");
   const int nsub = marfa_num_subintervals(run->start_wv, run->end_wv);
   if (isub < 0 || isub >= nsub) return fail(msg, msg_len, MARFA_E_ARG, "subinterval %d outside [0, %d)", isub, nsub);
-  for (int64_t i = 1; i < n_lines; ++i)
-    if (!(rec_nu(lines, i) >= rec_nu(lines, i - 1))) return fail(msg, msg_len, MARFA_E_UNSORTED, "lines not sorted");
-
   // line window of subinterval isub: starting line (main.f90:196-248) and the
-  // lblScheme recurrence with capWV (LBL.f90:41-61, main.f90:138-144)
+  // lblScheme recurrence with capWV (LBL.f90:41-61, main.f90:138-144), by the
+  // binary searches of the regular path on the (sorted) records
   const double cut = run->cutoff;
-  int64_t line_idx = 0;
-  double start_line = rec_nu(lines, 0);
-  if (run->start_wv > cut) {
-    int64_t i = 0;
-    while (rec_nu(lines, i) <= run->start_wv - cut)
-      if (++i >= n_lines) return fail(msg, msg_len, MARFA_E_DB, "line list ends before start - cutoff");
-    line_idx = i;
-    start_line = rec_nu(lines, i);
+  std::vector<double> ws, we;
+  std::vector<int64_t> wl, wh;
+  int bad = -1;
+  if (plan_windows_of(RecordNu{lines}, n_lines, run->start_wv, isub + 1, cut, ws, we, wl, wh, bad)) {
+    if (bad < 0) return fail(msg, msg_len, MARFA_E_DB, "line list ends before start - cutoff");
+    return fail(msg, msg_len, MARFA_E_DB, "line list ends inside the window of subinterval %d", bad);
   }
-  double s = run->start_wv;
-  int64_t lo = 0, hi = 0;
-  for (int k = 0; k <= isub; ++k) {
-    const double ext_end = s + DELTA_WV + cut;
-    double cap = (s - cut) + DELTA_WV;
-    if (cap <= start_line) cap = start_line;
-    int64_t I = line_idx, next = line_idx;
-    for (;; ++I) {
-      if (I >= n_lines) return fail(msg, msg_len, MARFA_E_DB, "line list ends inside the window of subinterval %d", k);
-      const double v = rec_nu(lines, I);
-      if (v >= ext_end) break;
-      if (v <= cap) next = I;
-    }
-    lo = line_idx;
-    hi = I;
-    if (k < isub) {
-      line_idx = next;
-      s = s + DELTA_WV;
-    }
-  }
+  const double s = ws[isub];
+  const int64_t lo = wl[isub], hi = wh[isub];
+  // the searches assume sorted centres; the records the window uses (and the
+  // one that ends it) are checked
+  for (int64_t i = std::max<int64_t>(lo, 1); i <= hi; ++i)
+    if (!(rec_nu(lines, i) >= rec_nu(lines, i - 1))) return fail(msg, msg_len, MARFA_E_UNSORTED, "lines not sorted");
   const int64_t m = hi - lo;
   if (m > MAXL)
     return fail(msg, msg_len, MARFA_E_CAPACITY, "window of %lld lines exceeds the static capacity of %lld lines",
@@ -208,20 +200,16 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
     return rc == MARFA_OK;
   };
 
-  // inputs: window line records (one strided copy per field), TIPS, tables
+  // inputs: the window's records in one copy (into the per-line parameter
+  // region, which the prep kernel writes only after the split), TIPS, tables
   double *d_nu = (double *)(base + OFF_NU);
   float *d_f32 = (float *)(base + OFF_F32);
   int *d_iso = (int *)(base + OFF_ISO);
-  const marfa_line_record *w = lines + lo;
-  const size_t rs = sizeof(marfa_line_record);
+  static_assert(sizeof(marfa_line_record) == 36 && 36 <= sizeof(LineGen), "record copy fits the parameter region");
   if (m > 0) {
-    if (!ck(cudaMemcpy2DAsync(d_nu, 8, &w->nu, rs, 8, m, cudaMemcpyHostToDevice, st), "h2d nu")) return rc;
-    const float *fields[6] = {&w->S, &w->gamma_air, &w->gamma_self, &w->e_lower, &w->n_air, &w->delta_air};
-    for (int f = 0; f < 6; ++f)
-      if (!ck(cudaMemcpy2DAsync(d_f32 + f * MAXL, 4, fields[f], rs, 4, m, cudaMemcpyHostToDevice, st), "h2d lines"))
-        return rc;
-    // jointMolIso as stored; divided by 100 on the device (iso_from_joint)
-    if (!ck(cudaMemcpy2DAsync(d_iso, 4, &w->joint_mol_iso, rs, 4, m, cudaMemcpyHostToDevice, st), "h2d iso"))
+    if (!ck(cudaMemcpyAsync(base + OFF_GEN, lines + lo, (size_t)m * sizeof(marfa_line_record),
+                            cudaMemcpyHostToDevice, st), "h2d lines") ||
+        !ck(split_records(base + OFF_GEN, m, d_nu, d_f32, d_iso, MAXL, st), "split records"))
       return rc;
   }
   double *d_tips = (double *)(base + OFF_TIPS);
@@ -290,7 +278,6 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   pp.hot64 = f64 ? (Hot64 *)(base + OFF_HOT) : nullptr;
   pp.err = &d_small->err;
   if (m > 0) {
-    if (!ck(iso_from_joint(d_iso, m, st), "iso kernel")) return rc;
     if (!ck(launch_prep(pp, st), "prep")) return rc;
     SortParams sp;
     sp.nu = d_nu;
