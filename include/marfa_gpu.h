@@ -44,9 +44,12 @@ extern "C" {
 #define MARFA_E_NOMEM 101       /* device allocation failed                          */
 #define MARFA_E_NODEVICE 110    /* no CUDA device                                    */
 
-/* line shapes (Shapes.f90:8-15).  ONE and ABSX are diagnostic shapes
- * (F = 1 and F = |X|) used to check the multigrid placement exactly. */
+/* line shapes (Shapes.f90:8-15): VOIGT is `voigt` (Shapes.f90:22-133),
+ * LORENTZ is `lorentzShape` (Shapes.f90:135-141), the chi-corrected Lorentz
+ * at every offset.  ONE and ABSX are diagnostic shapes (F = 1 and F = |X|)
+ * used to check the multigrid placement exactly. */
 #define MARFA_SHAPE_VOIGT 0
+#define MARFA_SHAPE_LORENTZ 1
 #define MARFA_SHAPE_ONE 100
 #define MARFA_SHAPE_ABSX 101
 
@@ -105,6 +108,19 @@ int marfa_ctx_create(const marfa_line_record *lines, int64_t n_lines, const doub
                      int n_iso, int n_temp, int device, marfa_ctx **out);
 void marfa_ctx_destroy(marfa_ctx *ctx);
 const char *marfa_last_error(const marfa_ctx *ctx);
+
+/* Temperature grid of the context's TIPS table: node j (0-based) at
+ * t_first + j * t_step K.  The default, 20 K and 2 K, is the grid of the
+ * reference's table (TIPS(74, 501), Gamache 2017; Spectroscopy.f90:91-115).
+ * The reference plans Gamache's 2021 partition sums (README.md:458-460),
+ * which come on 1 K steps: pass such a table as `tips` to marfa_ctx_create
+ * (isotopologues as rows, NaN beyond an isotopologue's last temperature) and
+ * set its grid here.  Q(T) is interpolated linearly between the nodes around
+ * T, as the reference does on its grid, and Q(296 K) is the node at 296 K
+ * when there is one.  296 K must lie inside the table (else MARFA_E_ARG);
+ * a level temperature outside it returns MARFA_E_TEMPERATURE.  Graphs
+ * captured before the change are refused afterwards (status 10). */
+int marfa_ctx_set_tips_grid(marfa_ctx *ctx, double t_first, double t_step);
 
 /* Number of subintervals of [start_wv, end_wv) (main.f90:117-122) and the
  * PT record number of subinterval `isub` (main.f90:126). */

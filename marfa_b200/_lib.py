@@ -11,7 +11,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libmarfa_gpu.so"
 
 MARFA_NT = 20481
-SHAPE = {"voigt": 0, "one": 100, "absx": 101}
+SHAPE = {"voigt": 0, "lorentz": 1, "one": 100, "absx": 101}
 CHI = {"none": 0, "tonkov": 1, "pollack": 2, "perrin": 3}
 TARGET = {"ACS": 0, "VAC": 1}
 PRECISION = {"fp64": 0, "fp32c": 1}
@@ -21,7 +21,7 @@ EXPORTS = (
     "marfa_ctx_create", "marfa_ctx_destroy", "marfa_last_error", "marfa_num_subintervals",
     "marfa_record_number", "marfa_compute", "marfa_compute_batched", "marfa_compute_device",
     "marfa_synchronize", "marfa_eval_count", "marfa_debug_accumulators", "marfa_last_timings",
-    "marfa_plan_windows", "marfa_compute_record_static",
+    "marfa_plan_windows", "marfa_compute_record_static", "marfa_ctx_set_tips_grid",
     "marfa_ctx_set_line_params", "marfa_vjp", "marfa_graph_create", "marfa_graph_launch",
     "marfa_graph_destroy", "marfa_autotune",
 )
@@ -76,6 +76,7 @@ def load():
         "marfa_compute_record_static": (I, [P, I64, P, I, I, ctypes.POINTER(MarfaRun), D, D, D, I, P,
                                             P, ctypes.c_char_p, ctypes.c_size_t]),
         "marfa_ctx_set_line_params": (I, [P, P, P]),
+        "marfa_ctx_set_tips_grid": (I, [P, D, D]),
         "marfa_vjp": (I, [P, ctypes.POINTER(MarfaRun), P, P, P, I, P, P, P, P, P]),
         "marfa_graph_create": (I, [P, ctypes.POINTER(MarfaRun), I, P, P, P, P, P, ctypes.POINTER(P)]),
         "marfa_graph_launch": (I, [P, P, P, P, P]),

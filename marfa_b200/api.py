@@ -186,6 +186,11 @@ class Context:
             self._h, ctypes.c_void_p(0 if self._S64 is None else self._S64.ctypes.data),
             ctypes.c_void_p(0 if self._g64 is None else self._g64.ctypes.data)))
 
+    def set_tips_grid(self, t_first: float, t_step: float):
+        """Temperature grid of the context's TIPS table (node j at t_first +
+        j t_step K; the reference's table: 20 K, 2 K)."""
+        self._check(self._lib.marfa_ctx_set_tips_grid(self._h, float(t_first), float(t_step)))
+
     def vjp(self, run: Run, pressure, temperature, density, cotangent) -> dict:
         """Vector-Jacobian product of the FP64 records for `cotangent`
         [n_levels, n_sub, 20481]: dict of dT, dP [n_levels] and dS,

@@ -249,15 +249,14 @@ __global__ void __launch_bounds__(256) adjoint_prep_kernel(AdjPrepParams p) {
     // pself = n 10 k T / p0 grows with T at fixed number density
     const double gamma = tf * (gair * (P - lv.pself) + gself * lv.pself);
     a.dg_dT = -nair / T * gamma + tf * (gself - gair) * (lv.pself / T);
-    const double tval = (T - 20.0) / 2.0 + 1.0;
-    const int idx = (int)tval;
-    if (tval >= 1.0 && idx + 1 <= p.n_temp) {
+    int idx = 1;
+    double uw = 0.0;
+    if (tips_node(T, p.tgrid, p.n_temp, idx, uw)) {
       const double *row = p.tips + (size_t)(iso - 1) * p.n_temp;
-      const double lwt = (double)idx * 2.0 + 18.0;
-      const double uw = (T - lwt) / 2.0, lw = 1.0 - uw;
+      const double lw = 1.0 - uw;
       const double Q = lw * row[idx - 1] + uw * row[idx];
-      const double dQ = (row[idx] - row[idx - 1]) / 2.0;
-      const double Qref = row[138];
+      const double dQ = (row[idx] - row[idx - 1]) / p.tgrid.dt;
+      const double Qref = tips_ref(row, p.tgrid, p.n_temp);
       const double E = (double)p.lines.elow[i];
       const double nu = p.lines.nu[i];
       const double boltz = exp(-(c.c2 * E / T)) / exp(-(c.c2 * E / c.tref));

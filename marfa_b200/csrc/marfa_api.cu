@@ -102,6 +102,7 @@ struct marfa_ctx {
   double smax = 0.0;       // largest reference intensity
   double dmin = 0.0, dmax = 0.0;
   int n_iso = 0, n_temp = 0;
+  TipsGrid tgrid{20.0, 2.0}; // the reference's TIPS grid unless set otherwise
   // line list, structure of arrays
   double *d_nu = nullptr;
   float *d_S = nullptr, *d_gair = nullptr, *d_gself = nullptr, *d_elow = nullptr,
@@ -312,7 +313,8 @@ int check_run(marfa_ctx *ctx, const marfa_run *run) {
     return set_err(ctx, 2, "target must be ACS or VAC");
   if (run->chi < MARFA_CHI_NONE || run->chi > MARFA_CHI_PERRIN)
     return set_err(ctx, MARFA_E_ARG, "unknown chi-factor %d", run->chi);
-  if (run->shape != MARFA_SHAPE_VOIGT && run->shape != MARFA_SHAPE_ONE && run->shape != MARFA_SHAPE_ABSX)
+  if (run->shape != MARFA_SHAPE_VOIGT && run->shape != MARFA_SHAPE_LORENTZ && run->shape != MARFA_SHAPE_ONE &&
+      run->shape != MARFA_SHAPE_ABSX)
     return set_err(ctx, MARFA_E_ARG, "unknown shape %d", run->shape);
   if (run->precision != MARFA_PREC_FP64 && run->precision != MARFA_PREC_FP32C)
     return set_err(ctx, MARFA_E_ARG, "unknown precision %d", run->precision);
@@ -327,9 +329,9 @@ int build_levels(marfa_ctx *ctx, int n, const double *P, const double *T, const 
   for (int l = 0; l < n; ++l) {
     if (!std::isfinite(P[l]) || !std::isfinite(T[l]) || !std::isfinite(dens[l]) || P[l] < 0.0)
       return set_err(ctx, 7, "level %d: invalid pressure/temperature/density", l + 1);
-    const double tval = (T[l] - 20.0) / 2.0 + 1.0;
-    const int idx = (int)tval;
-    if (!(tval >= 1.0) || idx + 1 > ctx->n_temp)
+    int idx = 1;
+    double uw = 0.0;
+    if (!tips_node(T[l], ctx->tgrid, ctx->n_temp, idx, uw))
       return set_err(ctx, MARFA_E_TEMPERATURE, "level %d: temperature %.3f K outside the TIPS table",
                      l + 1, T[l]);
     LevelConst &v = lv[l];
@@ -733,6 +735,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     pp.tips = ctx->d_tips;
     pp.n_iso = ctx->n_iso;
     pp.n_temp = ctx->n_temp;
+    pp.tgrid = ctx->tgrid;
     pp.lv = d_lv + l0;
     pp.n_levels = nl;
     pp.c = cst;
@@ -752,6 +755,7 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
       ap.tips = ctx->d_tips;
       ap.n_iso = ctx->n_iso;
       ap.n_temp = ctx->n_temp;
+      ap.tgrid = ctx->tgrid;
       ap.lv = pp.lv;
       ap.n_levels = nl;
       ap.c = cst;
@@ -1441,6 +1445,7 @@ int marfa_eval_count(marfa_ctx *ctx, const marfa_run *run, int n_levels, const d
       pp.tips = ctx->d_tips;
       pp.n_iso = ctx->n_iso;
       pp.n_temp = ctx->n_temp;
+      pp.tgrid = ctx->tgrid;
       pp.lv = (LevelConst *)ctx->b_lv.p + l;
       pp.n_levels = 1;
       pp.c = make_consts();
@@ -1493,6 +1498,22 @@ int marfa_debug_accumulators(marfa_ctx *ctx, const marfa_run *run, const double 
   } catch (...) {
     return set_err(ctx, MARFA_E_NOMEM, "host allocation failed");
   }
+}
+
+int marfa_ctx_set_tips_grid(marfa_ctx *ctx, double t_first, double t_step) {
+  if (!ctx) return MARFA_E_ARG;
+  if (!std::isfinite(t_first) || !std::isfinite(t_step) || !(t_step > 0.0))
+    return set_err(ctx, MARFA_E_ARG, "TIPS grid: bad first temperature %g or step %g", t_first, t_step);
+  const TipsGrid g{t_first, t_step};
+  int idx = 1;
+  double uw = 0.0;
+  const double k = (296.0 - t_first) / t_step;
+  const bool node = k >= 0.0 && k <= (double)(ctx->n_temp - 1) && (double)(int)k == k;
+  if (!node && !tips_node(296.0, g, ctx->n_temp, idx, uw))
+    return set_err(ctx, MARFA_E_ARG, "TIPS grid: 296 K outside the table of %d temperatures", ctx->n_temp);
+  ctx->tgrid = g;
+  ++ctx->alloc_gen; // captured graphs hold the old grid
+  return MARFA_OK;
 }
 
 int marfa_last_timings(marfa_ctx *ctx, double *times) {

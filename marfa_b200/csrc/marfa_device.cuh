@@ -77,6 +77,39 @@ struct LevelConst {
   double perrin_b1, perrin_b2; // perrin chi-factor temperature terms
 };
 
+// ------------------------------------------------------------------- TIPS
+// Temperature grid of the partition-sum table: node j (0-based) at
+// t0 + j dt.  The reference's table (TIPS(74, 501), Gamache 2017) has
+// t0 = 20 K, dt = 2 K; Gamache's 2021 tables use 1 K steps.
+struct TipsGrid {
+  double t0, dt;
+};
+
+// TIPSofT (Spectroscopy.f90:91-115): the lower node index idx (1-based, the
+// reference's `int((T - 20) / 2 + 1)`) and the weight uw of node idx + 1 for
+// linear interpolation, Q = (1 - uw) row[idx - 1] + uw row[idx]; false when T
+// lies outside the table.  On the reference's grid these are its operations.
+__host__ __device__ inline bool tips_node(double T, TipsGrid g, int n_temp, int &idx, double &uw) {
+  const double tval = (T - g.t0) / g.dt + 1.0;
+  if (!(tval >= 1.0) || !(tval < (double)n_temp)) return false; // idx + 1 <= n_temp
+  idx = (int)tval;
+  const double lwt = (double)(idx - 1) * g.dt + g.t0;
+  uw = (T - lwt) / g.dt;
+  return true;
+}
+
+// Q(296 K) of one row: the node itself when 296 K is a node (node 139 of the
+// reference's table, Spectroscopy.f90:136), else the interpolation there.
+__host__ __device__ inline double tips_ref(const double *row, TipsGrid g, int n_temp) {
+  const double k = (296.0 - g.t0) / g.dt;
+  const int ki = (int)k;
+  if ((double)ki == k) return row[ki];
+  int idx = 1;
+  double uw = 0.0;
+  tips_node(296.0, g, n_temp, idx, uw);
+  return (1.0 - uw) * row[idx - 1] + uw * row[idx];
+}
+
 // ---------------------------------------------------------------- Kahan sum
 struct Kahan {
   float s, c;

@@ -50,18 +50,17 @@ __global__ void __launch_bounds__(256) prep_kernel(PrepParams p) {
   const double gair = p.lines.gair64 ? p.lines.gair64[i] : (double)p.lines.gair[i];
   const double gamma = pow(c.tref / T, (double)p.lines.nair[i]) *
                        (gair * (P - lv.pself) + (double)p.lines.gself[i] * lv.pself);
-  // TIPSofT (Spectroscopy.f90:91-115): linear interpolation in 2 K steps
-  const double tval = (T - 20.0) / 2.0 + 1.0;
-  const int idx = (int)tval;
+  // TIPSofT (Spectroscopy.f90:91-115): linear interpolation on the table's grid
+  int idx = 1;
+  double uw = 0.0;
   double S = 0.0;
-  if (!(tval >= 1.0) || idx + 1 > p.n_temp) {
+  if (!tips_node(T, p.tgrid, p.n_temp, idx, uw)) {
     atomicMax(p.err, 11);
   } else {
     const double *row = p.tips + (size_t)(iso - 1) * p.n_temp;
-    const double lwt = (double)idx * 2.0 + 18.0;
-    const double uw = (T - lwt) / 2.0, lw = 1.0 - uw;
+    const double lw = 1.0 - uw;
     const double Q = lw * row[idx - 1] + uw * row[idx];
-    const double Qref = row[138];
+    const double Qref = tips_ref(row, p.tgrid, p.n_temp);
     if (!isfinite(Q) || !isfinite(Qref)) atomicMax(p.err, 13);
     // intensityOfT (Spectroscopy.f90:118-145), unshifted nu in the emission term
     const double E = (double)p.lines.elow[i];
@@ -387,7 +386,7 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
       bool left;
       if (!far_line(p.nus[lo + i], s, se, cut, D, left)) continue;
       const Hot64 h = p.hot64[lo + i];
-      if (p.shape == 0 && D * h.qx >= 15.0) {
+      if ((p.shape == 0 && D * h.qx >= 15.0) || p.shape == 1) { // lorentzShape: region 0 at every offset
         // every position in Lorentz region 0: gamma S / (pi (d^2 + gamma^2)) chi(d)
 #pragma unroll
         for (int k = 0; k < NFAR; ++k) {
@@ -431,7 +430,7 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
       bool left;
       if (!far_line(p.nus[lo + i], s, se, cut, D, left)) continue;
       const Hot32 h = p.hot32[lo + i];
-      if (p.shape == 0 && D * h.qx >= 15.0) {
+      if ((p.shape == 0 && D * h.qx >= 15.0) || p.shape == 1) { // lorentzShape: region 0 at every offset
         // Exact split of the double distance: D = N*2^-11 + f, so that
         // d_k = (N*2^-11 + k/2) + f is one correctly rounded float.
         const double Nd = floor(D * 2048.0);
@@ -541,12 +540,20 @@ struct NearStore {
   double sqrt14;
 
   // F(X) of line q: region 0 (chi-corrected Lorentz) inline, regions 1-4
-  // through the out-of-line voigt_core; diagnostic shapes are marked by qx < 0.
+  // through the out-of-line voigt_core; lorentzShape (qx = -2) and the
+  // diagnostic shapes are marked by qx < 0.
   template <int CHI>
   __device__ __forceinline__ Real evalc(int q, double X) const {
     const double ax = fabs(X);
     const double qxv = qx[q];
-    if (qxv < 0.0) return vy[q] < 0.0 ? (Real)1 : (Real)ax;
+    if (qxv < 0.0) { // lorentzShape (marked by qx = -2) or a diagnostic shape
+      if (qxv > -1.5) return vy[q] < 0.0 ? (Real)1 : (Real)ax;
+      const Real axr = (Real)ax;
+      const Real lor = fast_div(lorA[q], axr * axr + g2[q]);
+      if (CHI == CHI_NONE) return lor;
+      if (sizeof(Real) == 8) return lor * (Real)chi_factor_d<CHI>(ax, lv);
+      return lor * (Real)chi_factor_f<CHI>(ax, (float)ax, lv);
+    }
     if (ax * qxv >= 15.0) {
       const Real axr = (Real)ax;
       const Real lor = fast_div(lorA[q], axr * axr + g2[q]);
@@ -740,7 +747,11 @@ struct LineEval {
 
   __device__ __forceinline__ Real operator()(double X, const LevelConst &lv, double sqrt14) const {
     const double ax = fabs(X);
-    if (qx < 0.0) return vy < 0.0 ? (Real)1 : (Real)ax; // diagnostic shapes
+    if (qx < 0.0) { // diagnostic shapes, or lorentzShape (qx = -2; no chi below |X| = 3)
+      if (qx > -1.5) return vy < 0.0 ? (Real)1 : (Real)ax;
+      const Real axr = (Real)ax;
+      return fast_div(lorA, axr * axr + g2);
+    }
     const double VXd = ax * qx;
     if (VXd >= 15.0) {
       const Real axr = (Real)ax;
@@ -1125,7 +1136,7 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
     if (q < b) {
       li = sidx[q];
       keep = near_keep(snu[q], li, s, se, cut, wlo, whi, UU, cls);
-      if (keep && p.shape == 0) g = gen[li]; // in flight during the scan
+      if (keep && p.shape <= 1) g = gen[li]; // in flight during the scan
     }
     int tot;
     const int pos = m_total + block_excl_scan(keep, tot);
@@ -1135,9 +1146,9 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
       // bins of the centre lines (UU in [0, 10)): at most 20480
       n11[pos] = cls == 1 ? (short)(int)floor(UU * 2048.0) : (short)0;
       nv11[pos] = cls == 1 ? (short)(int)floor((DELTA_WV - UU) * 2048.0) : (short)0;
-      if (p.shape == 0) {
+      if (p.shape <= 1) {
         const ShapeP<Real> sp = shape_params<Real>(g, p.c, sscale);
-        st.qx[pos] = sp.qx;
+        st.qx[pos] = p.shape == 1 ? -2.0 : sp.qx; // -2 marks lorentzShape
         st.vy[pos] = sp.vy;
         st.lorA[pos] = sp.lorA;
         st.g2[pos] = sp.g2;

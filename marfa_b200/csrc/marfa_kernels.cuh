@@ -20,6 +20,7 @@ struct PrepParams {
   DeviceLines lines;
   const double *tips; // [n_iso][n_temp]
   int n_iso, n_temp;
+  TipsGrid tgrid;     // temperature grid of the table
   const LevelConst *lv; // [Lc]
   int n_levels;         // Lc
   Consts c;
@@ -144,6 +145,7 @@ struct AdjPrepParams {
   DeviceLines lines;
   const double *tips;
   int n_iso, n_temp;
+  TipsGrid tgrid;
   const LevelConst *lv;
   int n_levels;
   Consts c;

@@ -131,7 +131,8 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
     return fail(msg, msg_len, MARFA_E_CAPACITY, "TIPS table of %d x %d exceeds %zu values", n_iso, n_temp, TIPS_MAX);
   if (run->target != MARFA_TARGET_ACS && run->target != MARFA_TARGET_VAC) return fail(msg, msg_len, 2, "bad target");
   if (run->chi < 0 || run->chi > 3 || (run->precision != 0 && run->precision != 1) ||
-      (run->shape != 0 && run->shape != 100 && run->shape != 101) || !(run->cutoff > 0.0) || run->cutoff > 4000.0)
+      (run->shape != 0 && run->shape != 1 && run->shape != 100 && run->shape != 101) || !(run->cutoff > 0.0) ||
+      run->cutoff > 4000.0)
     return fail(msg, msg_len, MARFA_E_ARG, "bad run parameters");
   if (run->mol_code < 1 || run->mol_code > 12) return fail(msg, msg_len, 8, "unsupported molecule");
   const int nsub = marfa_num_subintervals(run->start_wv, run->end_wv);
@@ -169,8 +170,10 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   lv.pself = density * 10.0 * c.bolsi * temperature / c.stdp;
   lv.perrin_b1 = 0.0888 - 0.16 * std::exp(-(0.00410 * temperature));
   lv.perrin_b2 = 0.0526 * std::exp(-(0.00152 * temperature));
-  const double tval = (temperature - 20.0) / 2.0 + 1.0;
-  if (!(tval >= 1.0) || (int)tval + 1 > n_temp) return fail(msg, msg_len, MARFA_E_TEMPERATURE, "temperature outside TIPS");
+  int tidx = 1;
+  double tuw = 0.0;
+  if (!tips_node(temperature, TipsGrid{20.0, 2.0}, n_temp, tidx, tuw))
+    return fail(msg, msg_len, MARFA_E_TEMPERATURE, "temperature outside TIPS");
   if (!std::isfinite(pressure) || pressure < 0.0 || !std::isfinite(density) || lv.pself > pressure * (1.0 + 1e-6))
     return fail(msg, msg_len, 7, "invalid pressure / density");
   double dmin = 1e300, dmax = -1e300, smax = 0.0;
@@ -268,6 +271,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   pp.tips = d_tips;
   pp.n_iso = n_iso;
   pp.n_temp = n_temp;
+  pp.tgrid = TipsGrid{20.0, 2.0};
   pp.lv = &d_small->lv;
   pp.n_levels = 1;
   pp.c = c;

@@ -32,7 +32,7 @@ extern "C" {
 
 enum { ORACLE_MIXED = 0, ORACLE_FP64 = 1 };
 enum { ORACLE_CHI_NONE = 0, ORACLE_CHI_TONKOV = 1, ORACLE_CHI_POLLACK = 2, ORACLE_CHI_PERRIN = 3 };
-enum { ORACLE_SHAPE_VOIGT = 0, ORACLE_SHAPE_ONE = 100, ORACLE_SHAPE_ABSX = 101 };
+enum { ORACLE_SHAPE_VOIGT = 0, ORACLE_SHAPE_LORENTZ = 1, ORACLE_SHAPE_ONE = 100, ORACLE_SHAPE_ABSX = 101 };
 enum { ORACLE_TARGET_ACS = 0, ORACLE_TARGET_VAC = 1 };
 
 /* Layout of one (level, subinterval) accumulator dump (doubles):
@@ -47,8 +47,9 @@ enum { ORACLE_TARGET_ACS = 0, ORACLE_TARGET_VAC = 1 };
 typedef struct {
   const void *records;     /* n_lines 36-byte little-endian line records        */
   int64_t n_lines;
-  const double *tips;      /* [n_iso][n_temp] partition sums, T = 20 + 2*(j)   */
+  const double *tips;      /* [n_iso][n_temp] partition sums, T = t0 + dt*j    */
   int n_iso, n_temp;
+  double tips_t0, tips_dt; /* the table's grid (the reference's: 20 K, 2 K)    */
   const double *pressure;  /* [n_levels] atm                                   */
   const double *temperature;/* [n_levels] K                                    */
   const double *density;   /* [n_levels] molecules / (cm^2 km)                 */

@@ -21,7 +21,7 @@ NCELLS = 10230
 DUMP_LEN = NT + 3 * NCELLS
 MIXED, FP64 = 0, 1
 CHI = {"none": 0, "tonkov": 1, "pollack": 2, "perrin": 3}
-SHAPE = {"voigt": 0, "one": 100, "absx": 101}
+SHAPE = {"voigt": 0, "lorentz": 1, "one": 100, "absx": 101}
 TARGET = {"ACS": 0, "VAC": 1}
 
 
@@ -29,6 +29,7 @@ class OracleArgs(ctypes.Structure):
     _fields_ = [
         ("records", ctypes.c_void_p), ("n_lines", ctypes.c_int64),
         ("tips", ctypes.c_void_p), ("n_iso", ctypes.c_int), ("n_temp", ctypes.c_int),
+        ("tips_t0", ctypes.c_double), ("tips_dt", ctypes.c_double),
         ("pressure", ctypes.c_void_p), ("temperature", ctypes.c_void_p),
         ("density", ctypes.c_void_p), ("n_levels", ctypes.c_int),
         ("start_wv", ctypes.c_double), ("end_wv", ctypes.c_double),
@@ -74,7 +75,7 @@ class Oracle:
 
     def __init__(self, lines, tips, pressure, temperature, density, start_wv, end_wv,
                  cutoff, target="ACS", chi="none", mol_code=2, shape="voigt",
-                 precision=FP64, nthreads=None):
+                 precision=FP64, nthreads=None, tips_grid=(20.0, 2.0)):
         self.lines = np.ascontiguousarray(lines)
         assert self.lines.dtype.itemsize == 36
         self.tips = np.ascontiguousarray(tips, dtype=np.float64)
@@ -86,6 +87,7 @@ class Oracle:
         a.n_lines = len(self.lines)
         a.tips = self.tips.ctypes.data
         a.n_iso, a.n_temp = self.tips.shape
+        a.tips_t0, a.tips_dt = float(tips_grid[0]), float(tips_grid[1])
         a.pressure = self.P.ctypes.data
         a.temperature = self.T.ctypes.data
         a.density = self.n.ctypes.data

@@ -290,13 +290,15 @@ static real SFX(voigt)(work_t *w, double X) {
   }
 }
 
-/* FSHAPE: shapeFuncPtr => voigt (Shapes.f90:11-15) plus two diagnostic
+/* FSHAPE: shapeFuncPtr => voigt (Shapes.f90:11-15) or lorentzShape
+ * (Shapes.f90:135-141: chiCorrectedLorentz(X, lorHWHM)), plus two diagnostic
  * shapes used by placement tests (constant 1, and |X|). */
 static inline real SFX(fshape)(work_t *w, double X) {
   real v;
   w->evals++;
   if (w->shape == ORACLE_SHAPE_ONE) return RL(1.);
   if (w->shape == ORACLE_SHAPE_ABSX) return (real)fabs(X);
+  if (w->shape == ORACLE_SHAPE_LORENTZ) return SFX(chi_lorentz)(w, X, w->lorHWHM);
   v = SFX(voigt)(w, X);
   if (v < RL(0.)) w->negative_shape++;
   return v;
@@ -605,7 +607,8 @@ static int SFX(prepare_line)(work_t *w, const oracle_args *a, const level_t *lv,
                              const line_t *ln, double *nu_shift) {
   const consts_t *c = &w->c;
   int iso = ln->jmi / 100;
-  real molar, T = lv->temperature, Q, Qref, tips_factor, boltz, emis, lwt, lw, uw, tval;
+  real molar, T = lv->temperature, Q, Qref, tips_factor, boltz, emis, lwt, lw, uw, tval, t0, dt;
+  double k296;
   int idx;
   double nus;
   if (iso < 1 || iso > MARFA_WISO_LEN || iso > a->n_iso) return 13;
@@ -618,16 +621,29 @@ static int SFX(prepare_line)(work_t *w, const oracle_args *a, const level_t *lv,
   /* lorentzHWHM */
   w->lorHWHM = r_pow(c->TREF / T, ln->nair) *
                (ln->gair * (lv->pressure - lv->pSelf) + ln->gself * lv->pSelf);
-  /* TIPSofT */
-  tval = (T - RL(20.0)) / RL(2.) + RL(1.);
+  /* TIPSofT on the table's grid; on the reference's (20 K, 2 K) these are
+   * its operations: tval = (T - 20) / 2 + 1, lwt = idx * 2 + 18, and
+   * Q(296) = TIPS(iso, 139) */
+  t0 = (real)a->tips_t0;
+  dt = (real)a->tips_dt;
+  tval = (T - t0) / dt + RL(1.);
+  if (!(tval >= RL(1.)) || !(tval < (real)a->n_temp)) return 11;
   idx = (int)tval;
-  if (!(tval >= RL(1.)) || idx + 1 > a->n_temp) return 11;
-  lwt = (real)idx * RL(2.0) + RL(18.);
-  uw = (T - lwt) / RL(2.);
+  lwt = (real)(idx - 1) * dt + t0;
+  uw = (T - lwt) / dt;
   lw = RL(1.) - uw;
   Q = lw * (real)a->tips[(size_t)(iso - 1) * a->n_temp + (idx - 1)] +
       uw * (real)a->tips[(size_t)(iso - 1) * a->n_temp + idx];
-  Qref = (real)a->tips[(size_t)(iso - 1) * a->n_temp + 138];
+  k296 = (a->tips_dt > 0.0) ? (296.0 - a->tips_t0) / a->tips_dt : -1.0;
+  if (k296 >= 0.0 && k296 == (double)(int)k296 && (int)k296 < a->n_temp) {
+    Qref = (real)a->tips[(size_t)(iso - 1) * a->n_temp + (int)k296];
+  } else { /* 296 K between two nodes */
+    real tr = (RL(296.) - t0) / dt + RL(1.);
+    int ir = (int)tr;
+    real ur = (RL(296.) - ((real)(ir - 1) * dt + t0)) / dt;
+    Qref = (RL(1.) - ur) * (real)a->tips[(size_t)(iso - 1) * a->n_temp + (ir - 1)] +
+           ur * (real)a->tips[(size_t)(iso - 1) * a->n_temp + ir];
+  }
   /* intensityOfT (uses the unshifted nu) */
   tips_factor = Qref / Q;
   boltz = r_exp(-(c->C2 * ln->E / T)) / r_exp(-(c->C2 * ln->E / c->TREF));

@@ -210,3 +210,21 @@ def test_cascade_restatement_used_by_the_fp32c_check(cfg0, tips):
     for isub in (0, 5, 9):
         _, rk = tainted_points(o.accumulators(0, isub), want_record=True)
         assert np.max(np.abs(rk - rec[isub]) / rec[isub]) < 1e-13
+
+
+def test_tips_grid_resampled_to_1k_steps(tips):
+    """The oracle's TIPSofT on a 1 K grid, with the 2 K table resampled so
+    that linear interpolation gives the same partition sums, reproduces the
+    reference grid's records (all-double map)."""
+    w = synth.config(0, scale=0.25)
+    t = np.asarray(tips, dtype=np.float64)
+    t1 = np.empty((t.shape[0], 2 * t.shape[1] - 1))
+    t1[:, 0::2] = t
+    t1[:, 1::2] = 0.5 * (t[:, :-1] + t[:, 1:])
+    P, T = synth.f32([1.0]), synth.f32([251.3])
+    n = synth.ideal_gas_density(P, T)
+    kw = dict(target="ACS", chi="none", precision=O.FP64)
+    a = O.Oracle(w.lines, t, P, T, n, w.start_wv, w.end_wv, w.cutoff, **kw).run()[1]
+    b = O.Oracle(w.lines, t1, P, T, n, w.start_wv, w.end_wv, w.cutoff, tips_grid=(20.0, 1.0), **kw).run()[1]
+    m = a > 0
+    assert np.max(np.abs(a[m] - b[m]) / a[m]) <= 1e-12
