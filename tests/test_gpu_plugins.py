@@ -81,9 +81,10 @@ def test_tips_on_1k_grid(gpu, tips):
         with pytest.raises(MarfaError) as e:          # 296 K outside a table starting at 300 K
             ctx.set_tips_grid(300.0, 1.0)
         assert e.value.code == 10
-        hot = synth.Profile(synth.f32([1.0]), synth.f32([1001.0]),
-                            synth.ideal_gas_density(synth.f32([1.0]), synth.f32([1001.0])))
-        with pytest.raises(MarfaError) as e:          # beyond the last node (1000 K)
+        t_hot = 20.0 + (t1.shape[1] - 1) + 1.0      # 1 K past the table's last node
+        hot = synth.Profile(synth.f32([1.0]), synth.f32([t_hot]),
+                            synth.ideal_gas_density(synth.f32([1.0]), synth.f32([t_hot])))
+        with pytest.raises(MarfaError) as e:          # beyond the last node
             ctx.compute(run, hot.pressure, hot.temperature, hot.density)
         assert e.value.code == 11
     orc = O.Oracle(w.lines, t1, prof.pressure, prof.temperature, prof.density, w.start_wv, w.end_wv,
