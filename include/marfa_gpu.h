@@ -262,7 +262,8 @@ int marfa_last_timings(marfa_ctx *ctx, double *times);
  *   (it synchronises the stream and copies from pageable host memory, so it
  *   cannot be called on a stream that is being captured into a graph).
  *   msg (optional): receives a text description of a failure.
- * The first call on each device looks up the array's device address.  Every
+ * Every call looks up the array's device address on the current device (the
+ * first call on a device also loads the library's device code there).  Every
  * call on a device reuses the same array: calls that overlap on the GPU
  * (from two host threads, or on two streams) race, so callers serialise
  * them. */

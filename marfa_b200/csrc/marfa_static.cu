@@ -20,7 +20,6 @@
 // the array and leaves its contents behind for the next call; calls that
 // overlap on the GPU (two host threads, or two streams) race on it.
 #include <algorithm>
-#include <mutex>
 
 #include <cmath>
 #include <cstdarg>
@@ -69,9 +68,6 @@ static __device__ __align__(256) unsigned char g_static_scratch[MARFA_STATIC_SCR
 
 namespace {
 
-std::mutex g_addr_mu;
-unsigned char *g_addr[256] = {};
-
 int fail(char *msg, size_t len, int code, const char *fmt, ...) {
   if (msg && len) {
     va_list ap;
@@ -82,18 +78,18 @@ int fail(char *msg, size_t len, int code, const char *fmt, ...) {
   return code;
 }
 
-// device address of g_static_scratch on the current device (looked up once)
+// Device address of g_static_scratch on the current device.  In host code
+// the array's name stands for a host-side shadow, not a device address, so
+// the address is looked up with the device current -- on every call (a table
+// lookup in the runtime once its module is loaded; it allocates nothing), so
+// that it stays right after a cudaDeviceReset.
 int scratch_address(int dev, unsigned char **out, char *msg, size_t len) {
-  if (dev < 0 || dev >= 256) return fail(msg, len, MARFA_E_ARG, "device index %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_addr_mu);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess)
-      return fail(msg, len, MARFA_E_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(e));
-    g_addr[dev] = (unsigned char *)p;
-  }
-  *out = g_addr[dev];
+  if (dev < 0) return fail(msg, len, MARFA_E_ARG, "device index %d out of range", dev);
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess)
+    return fail(msg, len, MARFA_E_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(e));
+  *out = (unsigned char *)p;
   return MARFA_OK;
 }
 
