@@ -447,23 +447,77 @@ static void order_by_bound(const int *nb, int n, int *out, std::vector<int> &tmp
   for (int i = 0; i < n; ++i) out[cnt[key(tmp[i]) >> 8]++] = tmp[i];
 }
 
-// The whole computation for a flat list of levels.
-int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *P,
-               const double *T, const double *dens, const Outputs &o, cudaStream_t st) {
-  int rc = check_run(ctx, run);
-  if (rc) return rc;
-  if (n_levels < 1 || !P || !T || !dens) return set_err(ctx, MARFA_E_ARG, "no levels");
-  Plan pl;
-  if ((rc = make_plan(ctx, run, pl))) return rc;
-  std::vector<LevelConst> lv;
-  if ((rc = build_levels(ctx, n_levels, P, T, dens, lv))) return rc;
+// What one call of run_levels decides before it launches anything: the
+// precision form, the chunks of levels and their fine-kernel plans, the work
+// order of the units, the device tables.
+struct CallPlan {
+  int nsub = 0, C = 0, chi = MARFA_CHI_NONE;
+  int64_t N = 0;
+  bool f64 = false, adj = false, host_records = false, two = false;
+  Consts cst{};
+  double sscale = 1.0;                 // FP32c intensity scale
+  size_t elem = 4;                     // bytes per accumulator
+  int Lc = 0, UB = 0;                  // levels per chunk, units per fine/cascade batch
+  int n_chunks = 0;
+  std::vector<int> lb;                 // chunk c holds levels [lb[c], lb[c + 1])
+  std::vector<int> order;              // work-queue order of the units of every batch
+  std::vector<FineChunk> fine;         // fine-kernel launch plan per chunk
+  std::vector<double> margin;          // window margin per level
+  std::vector<long long> sig;          // the launch plan, for graph replays
+  double *d_s = nullptr, *d_e = nullptr;       // device window table
+  int64_t *d_lo = nullptr, *d_hi = nullptr;
+  int *d_sc0 = nullptr;
+  int64_t *d_cb = nullptr, *d_ce = nullptr;    // device far-chunk table
+  int *d_cs = nullptr;
+  LevelConst *d_lv = nullptr;
+  double *d_margin = nullptr;
+};
+
+// Timing events of every kernel family of one call, resolved by
+// marfa_last_timings (none inside a graph capture).
+struct Timeline {
+  marfa_ctx *ctx;
+  bool off;
+  size_t used = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> copies; // record copies
+  cudaEvent_t next() {
+    if (off) return nullptr;
+    if (used == ctx->events.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      ctx->events.push_back(e);
+    }
+    return ctx->events[used++];
+  }
+  void mark(int fam, cudaEvent_t a, cudaEvent_t b) { ctx->marks.push_back({fam, {a, b}}); }
+};
+
+// The per-chunk device buffers: set 1 is the second stream's copy.
+struct ChunkBufs {
+  DevBuf *nus, *gen, *hot, *rank, *snu, *sidx, *far, *scr, *gstage, *vbuf, *queue;
+};
+static ChunkBufs chunk_bufs(marfa_ctx *ctx, int set) {
+  if (set)
+    return {&ctx->b2_nus, &ctx->b2_gen, &ctx->b2_hot, &ctx->b2_rank, &ctx->b2_snu, &ctx->b2_sidx, &ctx->b2_far,
+            &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue};
+  return {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far, &ctx->b_scr,
+          &ctx->b_gstage, &ctx->b_vbuf, &ctx->b_queue};
+}
+
+// Precision constants, the memory plan (levels per chunk, units per batch)
+// and the chunks of levels; creates the streams and events the call needs.
+static int plan_call(marfa_ctx *ctx, const marfa_run *run, int n_levels, const Outputs &o, const Plan &pl,
+                     CallPlan &cp) {
   const int nsub = pl.n_sub;
-  if (nsub == 0) return MARFA_OK;
   const int64_t N = ctx->n_lines;
   const bool f64 = run->precision == MARFA_PREC_FP64;
-  const int chi = run->mol_code == 2 ? run->chi : MARFA_CHI_NONE; // CO2-only factors
   const int C = (int)pl.chunk_sub.size();
-  const Consts cst = make_consts();
+  cp.nsub = nsub;
+  cp.N = N;
+  cp.f64 = f64;
+  cp.C = C;
+  cp.chi = run->mol_code == 2 ? run->chi : MARFA_CHI_NONE; // CO2-only factors
+  cp.cst = make_consts();
 
   // FP32-compensated form: scale intensities by 2^E so that every partial
   // sum stays far from the float underflow and overflow limits.
@@ -527,7 +581,25 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     if (!ctx->fork_ev) CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming), "event");
     if (!ctx->join_ev) CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming), "event");
   }
+  cp.sscale = sscale;
+  cp.adj = adj;
+  cp.elem = elem;
+  cp.Lc = Lc;
+  cp.UB = UB;
+  cp.host_records = host_records;
+  cp.two = two;
+  cp.lb = lb;
+  cp.n_chunks = n_chunks;
+  return MARFA_OK;
+}
 
+// The call's device buffers (grown, never shrunk), the addresses of its
+// window and chunk tables and the window margin of every level.
+static int alloc_buffers(marfa_ctx *ctx, int n_levels, const double *P, const Outputs &o, CallPlan &cp) {
+  const int nsub = cp.nsub, C = cp.C, Lc = cp.Lc, UB = cp.UB;
+  const int64_t N = cp.N;
+  const bool f64 = cp.f64, adj = cp.adj, two = cp.two;
+  const size_t elem = cp.elem;
   CK(ensure(ctx, ctx->b_nus, (size_t)Lc * N * 8), "alloc nus");
   CK(ensure(ctx, ctx->b_gen, (size_t)Lc * N * sizeof(LineGen)), "alloc gen");
   CK(ensure(ctx, ctx->b_hot, (size_t)Lc * N * (f64 ? sizeof(Hot64) : sizeof(Hot32))), "alloc hot");
@@ -578,7 +650,30 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   }
   LevelConst *d_lv = (LevelConst *)ctx->b_lv.p;
   double *d_margin = (double *)ctx->b_margin.p;
+  cp.d_s = d_s;
+  cp.d_e = d_e;
+  cp.d_lo = d_lo;
+  cp.d_hi = d_hi;
+  cp.d_sc0 = d_sc0;
+  cp.d_cb = d_cb;
+  cp.d_ce = d_ce;
+  cp.d_cs = d_cs;
+  cp.margin = std::move(margin);
+  cp.d_lv = d_lv;
+  cp.d_margin = d_margin;
+  return MARFA_OK;
+}
 
+// Near-line bound and work order of every unit, the fine kernel's launch
+// plan per chunk of levels (with the staging and slot buffers it needs), and
+// the signature of the whole launch plan.
+static int plan_fine(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *P, const Plan &pl,
+                     CallPlan &cp) {
+  const int nsub = cp.nsub, chi = cp.chi, Lc = cp.Lc, UB = cp.UB, n_chunks = cp.n_chunks;
+  const int64_t N = cp.N;
+  const bool f64 = cp.f64, two = cp.two;
+  const size_t elem = cp.elem;
+  const std::vector<int> &lb = cp.lb;
   // Near-line bound of every unit, from the unshifted centres: a near line
   // has s - 1 < nu' < s + 11 (the bounds of fine_kernel) and nu' = nu + delta
   // P with delta in [dmin, dmax], so nu lies in (s - 1 - dmax P, s + 11 -
@@ -651,7 +746,22 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   sig.insert(sig.end(), lb.begin(), lb.end());
   for (const FineChunk &fc : fchunks)
     sig.insert(sig.end(), {fc.smem_cap, fc.gstage_cap, fc.block_threads, (long long)fc.smem_room, fc.resident});
+  cp.order = std::move(order_all);
+  cp.fine = std::move(fchunks);
+  cp.sig = std::move(sig);
+  return MARFA_OK;
+}
 
+// The window, chunk, level and order tables, through the pinned staging ring.
+static int stage_tables(marfa_ctx *ctx, cudaStream_t st, int n_levels, const Plan &pl,
+                        const std::vector<LevelConst> &lv, const CallPlan &cp) {
+  const int nsub = cp.nsub, C = cp.C;
+  double *d_s = cp.d_s, *d_e = cp.d_e, *d_margin = cp.d_margin;
+  int64_t *d_lo = cp.d_lo, *d_hi = cp.d_hi, *d_cb = cp.d_cb, *d_ce = cp.d_ce;
+  int *d_sc0 = cp.d_sc0, *d_cs = cp.d_cs;
+  LevelConst *d_lv = cp.d_lv;
+  const std::vector<double> &margin = cp.margin;
+  const std::vector<int> &order_all = cp.order;
   Staging sg{ctx, st};
   const size_t stage_bytes = 4 * Staging::room((size_t)nsub * 8) + Staging::room((size_t)(nsub + 1) * 4) +
                              2 * Staging::room((size_t)C * 8) + Staging::room((size_t)C * 4) +
@@ -670,6 +780,268 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   CK(sg.put(d_margin, margin.data(), n_levels * 8), "h2d margin");
   CK(sg.put(ctx->b_order.p, order_all.data(), order_all.size() * 4), "h2d order");
   CK(sg.end(), "staging event");
+  return MARFA_OK;
+}
+
+// The launches of chunk c of levels, on its stream: prep (and the adjoint's
+// prep), sort, far kernel, then per batch of units the fine kernel and the
+// cascade (or the adjoint kernels), and the copy of the chunk's records.
+static int launch_chunk(marfa_ctx *ctx, const marfa_run *run, const Outputs &o, const Plan &pl,
+                        const CallPlan &cp, int c, cudaStream_t st, Timeline &tl) {
+  const int nsub = cp.nsub, C = cp.C, chi = cp.chi, Lc = cp.Lc, UB = cp.UB;
+  const int64_t N = cp.N;
+  const bool f64 = cp.f64, adj = cp.adj, two = cp.two, host_records = cp.host_records;
+  const Consts cst = cp.cst;
+  const double sscale = cp.sscale;
+  const std::vector<int> &lb = cp.lb;
+  const std::vector<FineChunk> &fchunks = cp.fine;
+  int *d_sc0 = cp.d_sc0, *d_cs = cp.d_cs;
+  int64_t *d_cb = cp.d_cb, *d_ce = cp.d_ce;
+  LevelConst *d_lv = cp.d_lv;
+  double *d_margin = cp.d_margin;
+  const WindowTable win{cp.d_s, cp.d_e, cp.d_lo, cp.d_hi, nsub};
+  DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N,
+                 ctx->d_S64, ctx->d_gair64};
+  auto next_event = [&]() { return tl.next(); };
+  auto mark = [&](int fam, cudaEvent_t a, cudaEvent_t b) { tl.mark(fam, a, b); };
+  auto &copy_marks = tl.copies;
+  const int l0 = lb[c], nl = lb[c + 1] - lb[c];
+  // chunk c runs on stream c % 2 with buffer set c % 2 (one of each
+  // without host records); chunk c - 2 used the same ones on the same stream
+  const int set = two ? (c & 1) : 0;
+  const ChunkBufs B = chunk_bufs(ctx, set);
+  cudaStream_t cs = set ? ctx->stream2 : st;
+  PrepParams pp;
+  pp.lines = dl;
+  pp.tips = ctx->d_tips;
+  pp.n_iso = ctx->n_iso;
+  pp.n_temp = ctx->n_temp;
+  pp.tgrid = ctx->tgrid;
+  pp.lv = d_lv + l0;
+  pp.n_levels = nl;
+  pp.c = cst;
+  pp.sscale = sscale;
+  pp.nus = (double *)B.nus->p;
+  pp.gen = (LineGen *)B.gen->p;
+  pp.hot32 = f64 ? nullptr : (Hot32 *)B.hot->p;
+  pp.hot64 = f64 ? (Hot64 *)B.hot->p : nullptr;
+  pp.err = ctx->d_err;
+  cudaEvent_t e0 = next_event(), e1 = next_event(), e2 = next_event(), e3 = next_event();
+  if (e0) cudaEventRecord(e0, cs);
+  CK(launch_prep(pp, cs), "prep kernel");
+  ctx->launches += 1;
+  if (adj) {
+    AdjPrepParams ap;
+    ap.lines = dl;
+    ap.tips = ctx->d_tips;
+    ap.n_iso = ctx->n_iso;
+    ap.n_temp = ctx->n_temp;
+    ap.tgrid = ctx->tgrid;
+    ap.lv = pp.lv;
+    ap.n_levels = nl;
+    ap.c = cst;
+    ap.aux = (LineAux *)ctx->b_aux.p;
+    CK(launch_adjoint_prep(ap, cs), "adjoint prep kernel");
+    ctx->launches += 1;
+  }
+  if (e1) cudaEventRecord(e1, cs);
+  SortParams sp;
+  sp.nu = ctx->d_nu;
+  sp.nus = pp.nus;
+  sp.margin = d_margin + l0;
+  sp.n = N;
+  sp.n_levels = nl;
+  sp.rank = (int64_t *)B.rank->p;
+  sp.snu = (double *)B.snu->p;
+  sp.sidx = (int *)B.sidx->p;
+  CK(launch_sort(sp, cs), "sort kernels");
+  ctx->launches += 2;
+  if (e2) cudaEventRecord(e2, cs);
+  FarParams fp;
+  fp.nus = pp.nus;
+  fp.hot32 = pp.hot32;
+  fp.hot64 = pp.hot64;
+  fp.gen = pp.gen;
+  fp.lv = pp.lv;
+  fp.win = win;
+  fp.chunk_sub = d_cs;
+  fp.chunk_begin = d_cb;
+  fp.chunk_end = d_ce;
+  fp.n_chunks = C;
+  fp.n_levels = nl;
+  fp.n_lines = N;
+  fp.cutoff = run->cutoff;
+  fp.sscale = sscale;
+  fp.shape = run->shape;
+  fp.c = cst;
+  fp.out = (double *)B.far->p;
+  CK(launch_far(fp, run->precision, chi, cs), "far kernel");
+  if (C > 0) {
+    ctx->launches += 1;
+    ctx->far_launches += 1;
+  }
+  if (e3) cudaEventRecord(e3, cs);
+  mark(0, e0, e1);
+  mark(1, e1, e2);
+  mark(2, e2, e3);
+
+  const int half = c & 1;
+  float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p + (size_t)half * Lc * nsub * NT;
+  // the half written now was copied out two chunks ago
+  if (host_records && c >= 2) CK(cudaStreamWaitEvent(cs, ctx->rec_copied[half], 0), "wait copy");
+  const int out_level0 = o.dev_out ? l0 : 0;
+  const int units = nl * nsub;
+  // near-line counts of this chunk's units size the fine kernel's staging
+  FineParams fn;
+  fn.snu = sp.snu;
+  fn.sidx = sp.sidx;
+  fn.gen = pp.gen;
+  fn.lv = pp.lv;
+  fn.win = win;
+  fn.n_lines = N;
+  fn.cutoff = run->cutoff;
+  fn.sscale = sscale;
+  fn.shape = run->shape;
+  fn.c = cst;
+  fn.scratch = B.scr->p;
+  fn.err = ctx->d_err;
+  const FineChunk &fc = fchunks[c];
+  const int max_near = fc.max_near;
+  fn.smem_cap = fc.smem_cap;
+  fn.gstage_cap = fc.gstage_cap;
+  fn.gstage_bytes = fc.gstage_bytes;
+  fn.gstage = fc.gstage_cap ? B.gstage->p : nullptr;
+  fn.block_threads = fc.block_threads;
+  fn.smem_room = fc.smem_room;
+  const int resident = fc.resident;
+  fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
+  fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
+  fn.vbuf = B.vbuf->p;
+  fn.queue = (int *)B.queue->p;
+  fn.coop_k = ctx->tune.coop_k;
+  const int UBc = UB;
+  for (int u0 = 0; u0 < units; u0 += UBc) {
+    const int nu_ = std::min(UBc, units - u0);
+    fn.unit0 = u0;
+    fn.n_units = nu_;
+    fn.order = (const int *)ctx->b_order.p + (size_t)l0 * nsub + u0;
+    fn.grid = std::min(resident, nu_);
+    cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
+    if (f0) cudaEventRecord(f0, cs);
+    CK(cudaMemsetAsync(fn.queue, 0, sizeof(int), cs), "memset queue");
+    CK(launch_fine(fn, run->precision, chi, cs), "fine kernel");
+    ctx->launches += 1;
+    if (f1) cudaEventRecord(f1, cs);
+    if (adj) {
+      CascadeAdjParams ca;
+      ca.scratch = (const double *)B.scr->p;
+      ca.far = fp.out;
+      ca.sub_chunk0 = d_sc0;
+      ca.lv = pp.lv;
+      ca.n_chunks = C;
+      ca.n_sub = nsub;
+      ca.unit0 = u0;
+      ca.n_units = nu_;
+      ca.level_out0 = l0;
+      ca.target = run->target;
+      ca.cot = o.vjp->cot;
+      ca.gscratch = (double *)ctx->b_gscr.p;
+      CK(launch_cascade_adjoint(ca, cs), "cascade adjoint kernel");
+      AdjointParams ad;
+      ad.snu = sp.snu;
+      ad.sidx = sp.sidx;
+      ad.nus = pp.nus;
+      ad.gen = pp.gen;
+      ad.aux = (const LineAux *)ctx->b_aux.p;
+      ad.lv = pp.lv;
+      ad.win = win;
+      ad.sub_chunk0 = d_sc0;
+      ad.chunk_begin = d_cb;
+      ad.chunk_end = d_ce;
+      ad.max_chunks = pl.max_chunks;
+      ad.n_lines = N;
+      ad.unit0 = u0;
+      ad.n_units = nu_;
+      ad.level_out0 = l0;
+      ad.cutoff = run->cutoff;
+      ad.c = cst;
+      ad.gscratch = (const double *)ctx->b_gscr.p;
+      ad.dS = o.vjp->dS;
+      ad.dgair = o.vjp->dgair;
+      ad.dT = o.vjp->dT;
+      ad.dP = o.vjp->dP;
+      CK(launch_line_adjoint(ad, chi, std::min(64, (max_near + 255) / 256), cs), "line adjoint kernels");
+      ctx->launches += 2 + (pl.max_chunks > 0 ? 1 : 0);
+      if (f2) cudaEventRecord(f2, cs);
+      mark(3, f0, f1);
+      mark(4, f1, f2);
+      continue;
+    }
+    CascadeParams cp;
+    cp.scratch = B.scr->p;
+    cp.far = fp.out;
+    cp.sub_chunk0 = d_sc0;
+    cp.lv = pp.lv;
+    cp.n_chunks = C;
+    cp.n_sub = nsub;
+    cp.unit0 = u0;
+    cp.n_units = nu_;
+    cp.level_out0 = out_level0;
+    cp.inv_sscale = 1.0 / sscale;
+    cp.target = run->target;
+    cp.out = out_base;
+    cp.out64 = o.host_out64 ? (double *)ctx->b_out64.p : nullptr;
+    cp.dump = nullptr;
+    cp.dump_unit = -1;
+    if (o.host_dump && o.dump_level >= l0 && o.dump_level < l0 + nl) {
+      cp.dump = (double *)ctx->b_dump.p;
+      cp.dump_unit = (o.dump_level - l0) * nsub + o.dump_sub;
+    }
+    CK(launch_cascade(cp, run->precision, cs), "cascade kernel");
+    ctx->launches += cp.dump ? 2 : 1;
+    if (f2) cudaEventRecord(f2, cs);
+    mark(3, f0, f1);
+    mark(4, f1, f2);
+  }
+  if (host_records) {
+    CK(cudaEventRecord(ctx->rec_ready[half], cs), "event");
+    CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->rec_ready[half], 0), "wait records");
+    cudaEvent_t c0 = next_event(), c1 = next_event();
+    if (c0) cudaEventRecord(c0, ctx->copy_stream);
+    CK(cudaMemcpyAsync(o.host_out + (size_t)l0 * nsub * NT, out_base, (size_t)nl * nsub * NT * 4,
+                       cudaMemcpyDeviceToHost, ctx->copy_stream), "d2h records");
+    if (c1) cudaEventRecord(c1, ctx->copy_stream);
+    if (c0 && c1) copy_marks.push_back({c0, c1});
+    CK(cudaEventRecord(ctx->rec_copied[half], ctx->copy_stream), "event");
+  }
+  if (o.host_out64)
+    CK(cudaMemcpyAsync(o.host_out64 + (size_t)l0 * nsub * NT, ctx->b_out64.p, (size_t)nl * nsub * NT * 8,
+                       cudaMemcpyDeviceToHost, cs), "d2h records64");
+  return MARFA_OK;
+}
+
+// The whole computation for a flat list of levels: plan, tables, then the
+// chunks of levels (on two streams when the records go to the host), then
+// the end of the call (graph instantiation, or synchronisation, the timing
+// of the record copies for the next call's chunks and the device status).
+int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *P,
+               const double *T, const double *dens, const Outputs &o, cudaStream_t st) {
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  if (n_levels < 1 || !P || !T || !dens) return set_err(ctx, MARFA_E_ARG, "no levels");
+  Plan pl;
+  if ((rc = make_plan(ctx, run, pl))) return rc;
+  std::vector<LevelConst> lv;
+  if ((rc = build_levels(ctx, n_levels, P, T, dens, lv))) return rc;
+  if (pl.n_sub == 0) return MARFA_OK;
+  CallPlan cp;
+  if ((rc = plan_call(ctx, run, n_levels, o, pl, cp))) return rc;
+  if ((rc = alloc_buffers(ctx, n_levels, P, o, cp))) return rc;
+  if ((rc = plan_fine(ctx, run, n_levels, P, pl, cp))) return rc;
+  if ((rc = stage_tables(ctx, st, n_levels, pl, lv, cp))) return rc;
+  const int Lc = cp.Lc, UB = cp.UB, n_chunks = cp.n_chunks;
+  const bool two = cp.two, host_records = cp.host_records;
+  const std::vector<long long> &sig = cp.sig;
   if (o.graph && o.graph->replay) {
     if (sig != o.graph->sig)
       return set_err(ctx, MARFA_E_ARG, "the graph was captured for another launch plan (line buffers grown or "
@@ -688,262 +1060,26 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
   }
   CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st), "memset err");
 
-  WindowTable win{d_s, d_e, d_lo, d_hi, nsub};
-  DeviceLines dl{ctx->d_nu, ctx->d_S, ctx->d_gair, ctx->d_gself, ctx->d_elow, ctx->d_nair, ctx->d_delta, ctx->d_iso, N,
-                 ctx->d_S64, ctx->d_gair64};
-
   // timing events of every kernel family, resolved by marfa_last_timings
   ctx->marks.clear();
   ctx->launches = 0;
   ctx->far_launches = 0;
-  auto mark = [&](int fam, cudaEvent_t a, cudaEvent_t b) { ctx->marks.push_back({fam, {a, b}}); };
-  size_t ev_used = 0;
-  auto next_event = [&]() -> cudaEvent_t {
-    if (o.graph) return nullptr; // no timing events inside a graph
-    if (ev_used == ctx->events.size()) {
-      cudaEvent_t e;
-      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
-      ctx->events.push_back(e);
-    }
-    return ctx->events[ev_used++];
-  };
-  cudaEvent_t ev_begin = next_event();
+  Timeline tl{ctx, o.graph != nullptr, 0, {}};
+  cudaEvent_t ev_begin = tl.next();
   if (ev_begin) cudaEventRecord(ev_begin, st);
-
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> copy_marks;
-  struct ChunkBufs {
-    DevBuf *nus, *gen, *hot, *rank, *snu, *sidx, *far, *scr, *gstage, *vbuf, *queue;
-  };
-  const ChunkBufs sets[2] = {
-      {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far, &ctx->b_scr,
-       &ctx->b_gstage, &ctx->b_vbuf, &ctx->b_queue},
-      {&ctx->b2_nus, &ctx->b2_gen, &ctx->b2_hot, &ctx->b2_rank, &ctx->b2_snu, &ctx->b2_sidx, &ctx->b2_far,
-       &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue}};
   if (two) { // the second stream starts after the tables and the error flag
     CK(cudaEventRecord(ctx->fork_ev, st), "event");
     CK(cudaStreamWaitEvent(ctx->stream2, ctx->fork_ev, 0), "fork");
   }
-  for (int c = 0; c < n_chunks; ++c) {
-    const int l0 = lb[c], nl = lb[c + 1] - lb[c];
-    // chunk c runs on stream c % 2 with buffer set c % 2 (one of each
-    // without host records); chunk c - 2 used the same ones on the same stream
-    const int set = two ? (c & 1) : 0;
-    const ChunkBufs &B = sets[set];
-    cudaStream_t cs = set ? ctx->stream2 : st;
-    PrepParams pp;
-    pp.lines = dl;
-    pp.tips = ctx->d_tips;
-    pp.n_iso = ctx->n_iso;
-    pp.n_temp = ctx->n_temp;
-    pp.tgrid = ctx->tgrid;
-    pp.lv = d_lv + l0;
-    pp.n_levels = nl;
-    pp.c = cst;
-    pp.sscale = sscale;
-    pp.nus = (double *)B.nus->p;
-    pp.gen = (LineGen *)B.gen->p;
-    pp.hot32 = f64 ? nullptr : (Hot32 *)B.hot->p;
-    pp.hot64 = f64 ? (Hot64 *)B.hot->p : nullptr;
-    pp.err = ctx->d_err;
-    cudaEvent_t e0 = next_event(), e1 = next_event(), e2 = next_event(), e3 = next_event();
-    if (e0) cudaEventRecord(e0, cs);
-    CK(launch_prep(pp, cs), "prep kernel");
-    ctx->launches += 1;
-    if (adj) {
-      AdjPrepParams ap;
-      ap.lines = dl;
-      ap.tips = ctx->d_tips;
-      ap.n_iso = ctx->n_iso;
-      ap.n_temp = ctx->n_temp;
-      ap.tgrid = ctx->tgrid;
-      ap.lv = pp.lv;
-      ap.n_levels = nl;
-      ap.c = cst;
-      ap.aux = (LineAux *)ctx->b_aux.p;
-      CK(launch_adjoint_prep(ap, cs), "adjoint prep kernel");
-      ctx->launches += 1;
-    }
-    if (e1) cudaEventRecord(e1, cs);
-    SortParams sp;
-    sp.nu = ctx->d_nu;
-    sp.nus = pp.nus;
-    sp.margin = d_margin + l0;
-    sp.n = N;
-    sp.n_levels = nl;
-    sp.rank = (int64_t *)B.rank->p;
-    sp.snu = (double *)B.snu->p;
-    sp.sidx = (int *)B.sidx->p;
-    CK(launch_sort(sp, cs), "sort kernels");
-    ctx->launches += 2;
-    if (e2) cudaEventRecord(e2, cs);
-    FarParams fp;
-    fp.nus = pp.nus;
-    fp.hot32 = pp.hot32;
-    fp.hot64 = pp.hot64;
-    fp.gen = pp.gen;
-    fp.lv = pp.lv;
-    fp.win = win;
-    fp.chunk_sub = d_cs;
-    fp.chunk_begin = d_cb;
-    fp.chunk_end = d_ce;
-    fp.n_chunks = C;
-    fp.n_levels = nl;
-    fp.n_lines = N;
-    fp.cutoff = run->cutoff;
-    fp.sscale = sscale;
-    fp.shape = run->shape;
-    fp.c = cst;
-    fp.out = (double *)B.far->p;
-    CK(launch_far(fp, run->precision, chi, cs), "far kernel");
-    if (C > 0) {
-      ctx->launches += 1;
-      ctx->far_launches += 1;
-    }
-    if (e3) cudaEventRecord(e3, cs);
-    mark(0, e0, e1);
-    mark(1, e1, e2);
-    mark(2, e2, e3);
-
-    const int half = c & 1;
-    float *out_base = o.dev_out ? o.dev_out : (float *)ctx->b_out.p + (size_t)half * Lc * nsub * NT;
-    // the half written now was copied out two chunks ago
-    if (host_records && c >= 2) CK(cudaStreamWaitEvent(cs, ctx->rec_copied[half], 0), "wait copy");
-    const int out_level0 = o.dev_out ? l0 : 0;
-    const int units = nl * nsub;
-    // near-line counts of this chunk's units size the fine kernel's staging
-    FineParams fn;
-    fn.snu = sp.snu;
-    fn.sidx = sp.sidx;
-    fn.gen = pp.gen;
-    fn.lv = pp.lv;
-    fn.win = win;
-    fn.n_lines = N;
-    fn.cutoff = run->cutoff;
-    fn.sscale = sscale;
-    fn.shape = run->shape;
-    fn.c = cst;
-    fn.scratch = B.scr->p;
-    fn.err = ctx->d_err;
-    const FineChunk &fc = fchunks[c];
-    const int max_near = fc.max_near;
-    fn.smem_cap = fc.smem_cap;
-    fn.gstage_cap = fc.gstage_cap;
-    fn.gstage_bytes = fc.gstage_bytes;
-    fn.gstage = fc.gstage_cap ? B.gstage->p : nullptr;
-    fn.block_threads = fc.block_threads;
-    fn.smem_room = fc.smem_room;
-    const int resident = fc.resident;
-    fn.vbuf_cap = std::max(fn.smem_cap, fn.gstage_cap);
-    fn.vbuf_stride = fine_vbuf_elems(fn.vbuf_cap);
-    fn.vbuf = B.vbuf->p;
-    fn.queue = (int *)B.queue->p;
-    fn.coop_k = ctx->tune.coop_k;
-    const int UBc = UB;
-    for (int u0 = 0; u0 < units; u0 += UBc) {
-      const int nu_ = std::min(UBc, units - u0);
-      fn.unit0 = u0;
-      fn.n_units = nu_;
-      fn.order = (const int *)ctx->b_order.p + (size_t)l0 * nsub + u0;
-      fn.grid = std::min(resident, nu_);
-      cudaEvent_t f0 = next_event(), f1 = next_event(), f2 = next_event();
-      if (f0) cudaEventRecord(f0, cs);
-      CK(cudaMemsetAsync(fn.queue, 0, sizeof(int), cs), "memset queue");
-      CK(launch_fine(fn, run->precision, chi, cs), "fine kernel");
-      ctx->launches += 1;
-      if (f1) cudaEventRecord(f1, cs);
-      if (adj) {
-        CascadeAdjParams ca;
-        ca.scratch = (const double *)B.scr->p;
-        ca.far = fp.out;
-        ca.sub_chunk0 = d_sc0;
-        ca.lv = pp.lv;
-        ca.n_chunks = C;
-        ca.n_sub = nsub;
-        ca.unit0 = u0;
-        ca.n_units = nu_;
-        ca.level_out0 = l0;
-        ca.target = run->target;
-        ca.cot = o.vjp->cot;
-        ca.gscratch = (double *)ctx->b_gscr.p;
-        CK(launch_cascade_adjoint(ca, cs), "cascade adjoint kernel");
-        AdjointParams ad;
-        ad.snu = sp.snu;
-        ad.sidx = sp.sidx;
-        ad.nus = pp.nus;
-        ad.gen = pp.gen;
-        ad.aux = (const LineAux *)ctx->b_aux.p;
-        ad.lv = pp.lv;
-        ad.win = win;
-        ad.sub_chunk0 = d_sc0;
-        ad.chunk_begin = d_cb;
-        ad.chunk_end = d_ce;
-        ad.max_chunks = pl.max_chunks;
-        ad.n_lines = N;
-        ad.unit0 = u0;
-        ad.n_units = nu_;
-        ad.level_out0 = l0;
-        ad.cutoff = run->cutoff;
-        ad.c = cst;
-        ad.gscratch = (const double *)ctx->b_gscr.p;
-        ad.dS = o.vjp->dS;
-        ad.dgair = o.vjp->dgair;
-        ad.dT = o.vjp->dT;
-        ad.dP = o.vjp->dP;
-        CK(launch_line_adjoint(ad, chi, std::min(64, (max_near + 255) / 256), cs), "line adjoint kernels");
-        ctx->launches += 2 + (pl.max_chunks > 0 ? 1 : 0);
-        if (f2) cudaEventRecord(f2, cs);
-        mark(3, f0, f1);
-        mark(4, f1, f2);
-        continue;
-      }
-      CascadeParams cp;
-      cp.scratch = B.scr->p;
-      cp.far = fp.out;
-      cp.sub_chunk0 = d_sc0;
-      cp.lv = pp.lv;
-      cp.n_chunks = C;
-      cp.n_sub = nsub;
-      cp.unit0 = u0;
-      cp.n_units = nu_;
-      cp.level_out0 = out_level0;
-      cp.inv_sscale = 1.0 / sscale;
-      cp.target = run->target;
-      cp.out = out_base;
-      cp.out64 = o.host_out64 ? (double *)ctx->b_out64.p : nullptr;
-      cp.dump = nullptr;
-      cp.dump_unit = -1;
-      if (o.host_dump && o.dump_level >= l0 && o.dump_level < l0 + nl) {
-        cp.dump = (double *)ctx->b_dump.p;
-        cp.dump_unit = (o.dump_level - l0) * nsub + o.dump_sub;
-      }
-      CK(launch_cascade(cp, run->precision, cs), "cascade kernel");
-      ctx->launches += cp.dump ? 2 : 1;
-      if (f2) cudaEventRecord(f2, cs);
-      mark(3, f0, f1);
-      mark(4, f1, f2);
-    }
-    if (host_records) {
-      CK(cudaEventRecord(ctx->rec_ready[half], cs), "event");
-      CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->rec_ready[half], 0), "wait records");
-      cudaEvent_t c0 = next_event(), c1 = next_event();
-      if (c0) cudaEventRecord(c0, ctx->copy_stream);
-      CK(cudaMemcpyAsync(o.host_out + (size_t)l0 * nsub * NT, out_base, (size_t)nl * nsub * NT * 4,
-                         cudaMemcpyDeviceToHost, ctx->copy_stream), "d2h records");
-      if (c1) cudaEventRecord(c1, ctx->copy_stream);
-      if (c0 && c1) copy_marks.push_back({c0, c1});
-      CK(cudaEventRecord(ctx->rec_copied[half], ctx->copy_stream), "event");
-    }
-    if (o.host_out64)
-      CK(cudaMemcpyAsync(o.host_out64 + (size_t)l0 * nsub * NT, ctx->b_out64.p, (size_t)nl * nsub * NT * 8,
-                         cudaMemcpyDeviceToHost, cs), "d2h records64");
-  }
+  for (int c = 0; c < n_chunks; ++c)
+    if ((rc = launch_chunk(ctx, run, o, pl, cp, c, st, tl))) return rc;
   if (two) { // join the second stream
     CK(cudaEventRecord(ctx->join_ev, ctx->stream2), "event");
     CK(cudaStreamWaitEvent(st, ctx->join_ev, 0), "join");
   }
-  cudaEvent_t ev_end = next_event();
+  cudaEvent_t ev_end = tl.next();
   if (ev_end) cudaEventRecord(ev_end, st);
-  if (ev_begin && ev_end) mark(5, ev_begin, ev_end);
+  if (ev_begin && ev_end) tl.mark(5, ev_begin, ev_end);
   if (o.host_dump)
     CK(cudaMemcpyAsync(o.host_dump, ctx->b_dump.p, (size_t)(NT + 3 * NCELLS) * 8, cudaMemcpyDeviceToHost, st),
        "d2h dump");
@@ -967,9 +1103,9 @@ int run_levels(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double 
     float ms = 0.f;
     for (auto &m : ctx->marks)
       if (m.first == 5 && cudaEventElapsedTime(&ms, m.second.first, m.second.second) == cudaSuccess) kms += ms;
-    for (auto &m : copy_marks)
+    for (auto &m : tl.copies)
       if (cudaEventElapsedTime(&ms, m.first, m.second) == cudaSuccess) cms += ms;
-    if (kms > 0.0 && cms > 0.0 && copy_marks.size() == (size_t)n_chunks) {
+    if (kms > 0.0 && cms > 0.0 && tl.copies.size() == (size_t)n_chunks) {
       ctx->rec_compute_ms = kms / n_levels;
       ctx->rec_copy_ms = cms / n_levels;
     }
