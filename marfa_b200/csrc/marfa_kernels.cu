@@ -382,8 +382,66 @@ struct FarAcc {
   }
 };
 
+// Asynchronous global -> shared copies (cp.async, sm_80+ form; no barrier or
+// mbarrier: a thread's cp.async.wait_group completes its own copies).
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+constexpr int FAR_TH = 256;    // threads per far-kernel block
+constexpr int FAR_STAGES = 3;  // line tiles in flight per block
+
+// The far kernel's line parameters (shifted centre and the hot record) staged
+// through shared memory by cp.async: tile k holds lines begin + 256 k + t, one
+// per thread t, in a ring of FAR_STAGES tiles, so the loads of the next two
+// tiles are in flight while a thread evaluates its line of this one.  Each
+// thread copies and later reads only its own line of a tile, so its own
+// wait_group orders the copy before the read, without a barrier.
+template <class Hot>
+struct FarTiles {
+  struct __align__(16) Tile {
+    double nu[FAR_TH];
+    Hot hot[FAR_TH];
+  };
+  static_assert(sizeof(Hot) == 16 || sizeof(Hot) == 24, "hot record of 16 or 24 bytes");
+  Tile *ring;
+  const double *nus;   // this level's shifted centres
+  const Hot *hot;      // this level's hot records
+  int64_t begin, end;  // the block's lines
+  // copies tile k (lines past the end copy nothing) and commits one group
+  __device__ __forceinline__ void issue(int k) const {
+    const int64_t i = begin + (int64_t)k * FAR_TH + threadIdx.x;
+    if (i < end) {
+      Tile &t = ring[k % FAR_STAGES];
+      cp_async8(&t.nu[threadIdx.x], nus + i);
+      if (sizeof(Hot) == 16) {
+        cp_async16(&t.hot[threadIdx.x], hot + i);
+      } else {
+        const double *src = (const double *)(hot + i);
+        double *dst = (double *)&t.hot[threadIdx.x];
+        cp_async8(dst, src);
+        cp_async8(dst + 1, src + 1);
+        cp_async8(dst + 2, src + 2);
+      }
+    }
+    cp_async_commit();
+  }
+  // tile k has arrived (the FAR_STAGES - 1 tiles after it may be in flight)
+  __device__ __forceinline__ void wait() const { cp_async_wait<FAR_STAGES - 1>(); }
+  __device__ __forceinline__ double nu(int k) const { return ring[k % FAR_STAGES].nu[threadIdx.x]; }
+  __device__ __forceinline__ Hot line(int k) const { return ring[k % FAR_STAGES].hot[threadIdx.x]; }
+};
+
 template <bool F64, int CHI>
-__global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
+__global__ void __launch_bounds__(FAR_TH, F64 ? 2 : 4) far_kernel(FarParams p) {
   const int item = blockIdx.x;
   const int l = item / p.n_chunks;
   const int ci = item - l * p.n_chunks;
@@ -392,16 +450,26 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
   const double s = p.win.sub_s[sub], se = p.win.sub_e[sub], cut = p.cutoff;
   const LevelConst lv = p.lv[l];
   const size_t lo = (size_t)l * p.n_lines;
+  using HotT = typename std::conditional<F64, Hot64, Hot32>::type;
+  __shared__ typename FarTiles<HotT>::Tile ring[FAR_STAGES];
+  const FarTiles<HotT> tiles{ring, p.nus + lo, (const HotT *)(F64 ? (const void *)p.hot64 : (const void *)p.hot32) + lo,
+                             begin, end};
+  const int ntile = (int)((end - begin + FAR_TH - 1) / FAR_TH);
+#pragma unroll
+  for (int k = 0; k < FAR_STAGES - 1; ++k) tiles.issue(k);
   double res[NFAR];
-  if (F64) {
+  if constexpr (F64) {
     double acc[NFAR];
 #pragma unroll
     for (int k = 0; k < NFAR; ++k) acc[k] = 0.0;
-    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+    for (int k = 0; k < ntile; ++k) {
+      tiles.issue(k + FAR_STAGES - 1);
+      tiles.wait();
+      const int64_t i = begin + (int64_t)k * FAR_TH + threadIdx.x;
       double D;
       bool left;
-      if (!far_line(p.nus[lo + i], s, se, cut, D, left)) continue;
-      const Hot64 h = p.hot64[lo + i];
+      if (i >= end || !far_line(tiles.nu(k), s, se, cut, D, left)) continue;
+      const Hot64 h = tiles.line(k);
       if ((p.shape == 0 && D * h.qx >= 15.0) || p.shape == 1) { // lorentzShape: region 0 at every offset
         // every position in Lorentz region 0: gamma S / (pi (d^2 + gamma^2)) chi(d)
 #pragma unroll
@@ -441,11 +509,14 @@ __global__ void __launch_bounds__(256, F64 ? 2 : 4) far_kernel(FarParams p) {
     FarAcc fa;
     fa.init();
     const ChiPieces<CHI> pc(lv);
-    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+    for (int k = 0; k < ntile; ++k) {
+      tiles.issue(k + FAR_STAGES - 1);
+      tiles.wait();
+      const int64_t i = begin + (int64_t)k * FAR_TH + threadIdx.x;
       double D;
       bool left;
-      if (!far_line(p.nus[lo + i], s, se, cut, D, left)) continue;
-      const Hot32 h = p.hot32[lo + i];
+      if (i >= end || !far_line(tiles.nu(k), s, se, cut, D, left)) continue;
+      const Hot32 h = tiles.line(k);
       if ((p.shape == 0 && D * h.qx >= 15.0) || p.shape == 1) { // lorentzShape: region 0 at every offset
         // Exact split of the double distance: D = N*2^-11 + f, so that
         // d_k = (N*2^-11 + k/2) + f is one correctly rounded float.
@@ -1550,10 +1621,10 @@ cudaError_t launch_sort(const SortParams &p, cudaStream_t st) {
 template <bool F64>
 static void far_dispatch(const FarParams &p, int chi, unsigned nblk, cudaStream_t st) {
   switch (chi) {
-  case CHI_TONKOV: far_kernel<F64, CHI_TONKOV><<<nblk, 256, 0, st>>>(p); break;
-  case CHI_POLLACK: far_kernel<F64, CHI_POLLACK><<<nblk, 256, 0, st>>>(p); break;
-  case CHI_PERRIN: far_kernel<F64, CHI_PERRIN><<<nblk, 256, 0, st>>>(p); break;
-  default: far_kernel<F64, CHI_NONE><<<nblk, 256, 0, st>>>(p); break;
+  case CHI_TONKOV: far_kernel<F64, CHI_TONKOV><<<nblk, FAR_TH, 0, st>>>(p); break;
+  case CHI_POLLACK: far_kernel<F64, CHI_POLLACK><<<nblk, FAR_TH, 0, st>>>(p); break;
+  case CHI_PERRIN: far_kernel<F64, CHI_PERRIN><<<nblk, FAR_TH, 0, st>>>(p); break;
+  default: far_kernel<F64, CHI_NONE><<<nblk, FAR_TH, 0, st>>>(p); break;
   }
 }
 
