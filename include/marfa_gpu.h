@@ -191,12 +191,26 @@ void marfa_graph_destroy(marfa_graph *graph);
  * lines per far-kernel block (far_chunk: 2048, 4096, 8192 or 16384) and the number of
  * coarse fine grids whose accumulators are summed by groups of lanes rather
  * than one thread each (coop_k: 1..5) -- by timing every candidate on up to four levels of the given
- * profile, keeps the fastest in the context and returns it.  Results change
- * only by summation order (far-line sums are split differently).  No
- * reference counterpart (the reference has no launch parameters). */
+ * profile; for FP32c it then times the other fine-kernel block shape
+ * (fine_pair, see marfa_ctx_set_launch) at the best of those.  Keeps the
+ * fastest in the context and returns far_chunk and coop_k (the shape through
+ * marfa_ctx_get_launch).  Results change only by summation order (far-line
+ * sums are split differently).  No reference counterpart (the reference has
+ * no launch parameters). */
 int marfa_autotune(marfa_ctx *ctx, const marfa_run *run, int n_levels, const double *pressure,
                    const double *temperature, const double *density, int *far_chunk,
                    int *coop_k);
+
+/* Sets the context's launch parameters (as chosen by marfa_autotune, for
+ * example to reuse a tuning across processes): far_chunk (2048, 4096, 8192 or
+ * 16384), coop_k (1..5) and fine_pair (0: FP32c units with many near lines
+ * run on one 1024-thread fine block per SM; 1: on two 512-thread blocks per
+ * SM; FP64 ignores it).  Returns MARFA_E_ARG for any other value.  Graphs
+ * captured before the change keep their launch plan and are refused on
+ * replay when it differs. */
+int marfa_ctx_set_launch(marfa_ctx *ctx, int far_chunk, int coop_k, int fine_pair);
+/* The context's current launch parameters (any pointer may be NULL). */
+int marfa_ctx_get_launch(marfa_ctx *ctx, int *far_chunk, int *coop_k, int *fine_pair);
 
 /* Replaces the reference intensities S and air-broadening coefficients
  * gamma_air of every line by double values (either pointer may be NULL: back

@@ -23,7 +23,7 @@ EXPORTS = (
     "marfa_synchronize", "marfa_eval_count", "marfa_debug_accumulators", "marfa_last_timings",
     "marfa_plan_windows", "marfa_compute_record_static", "marfa_ctx_set_tips_grid",
     "marfa_ctx_set_line_params", "marfa_vjp", "marfa_graph_create", "marfa_graph_launch",
-    "marfa_graph_destroy", "marfa_autotune",
+    "marfa_graph_destroy", "marfa_autotune", "marfa_ctx_set_launch", "marfa_ctx_get_launch",
 )
 
 
@@ -82,6 +82,8 @@ def load():
         "marfa_graph_launch": (I, [P, P, P, P, P]),
         "marfa_graph_destroy": (None, [P]),
         "marfa_autotune": (I, [P, ctypes.POINTER(MarfaRun), I, P, P, P, P, P]),
+        "marfa_ctx_set_launch": (I, [P, I, I, I]),
+        "marfa_ctx_get_launch": (I, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -168,7 +168,20 @@ class Context:
         self._check(self._lib.marfa_autotune(self._h, ctypes.byref(r), len(P), P.ctypes.data,
                                              T.ctypes.data, n.ctypes.data, ctypes.byref(fc),
                                              ctypes.byref(ck)))
-        return {"far_chunk": fc.value, "coop_k": ck.value}
+        return self.launch()
+
+    def launch(self) -> dict:
+        """The context's launch parameters: lines per far-kernel block,
+        coarse fine grids summed by lane groups, and the FP32c fine-block
+        shape (0: one 1024-thread block per SM, 1: two of 512)."""
+        fc, ck, fp = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.marfa_ctx_get_launch(self._h, ctypes.byref(fc), ctypes.byref(ck),
+                                                   ctypes.byref(fp)))
+        return {"far_chunk": fc.value, "coop_k": ck.value, "fine_pair": fp.value}
+
+    def set_launch(self, far_chunk: int, coop_k: int, fine_pair: int) -> None:
+        """Pin the launch parameters (as returned by autotune or launch)."""
+        self._check(self._lib.marfa_ctx_set_launch(self._h, int(far_chunk), int(coop_k), int(fine_pair)))
 
     @property
     def n_lines(self) -> int:

@@ -36,6 +36,7 @@ struct Tune {
   int far_chunk = 16384;   // lines per far-kernel block
   int coop_k = 5;          // fine grids whose cell pairs are summed by lane groups
   int small_block_lines = 512; // batches whose units all have fewer near lines use small blocks
+  int fine_pair = 0;       // FP32c dense units on two 512-thread fine blocks per SM (else one of 1024)
 };
 
 // Bucket index over the sorted line centres: first[b] = first line with
@@ -717,7 +718,8 @@ static int plan_fine(marfa_ctx *ctx, const marfa_run *run, int n_levels, const d
     if (fc.max_near > 65535) // line indices of one unit are 16-bit in the fine kernel's bin table
       return set_err(ctx, MARFA_E_CAPACITY, "%d lines within 1 cm-1 of one subinterval (at most 65535)",
                      fc.max_near);
-    fc.block_threads = fine_block_threads(run->precision, fc.max_near, ctx->tune.small_block_lines);
+    fc.block_threads = fine_block_threads(run->precision, fc.max_near, ctx->tune.small_block_lines,
+                                          ctx->tune.fine_pair);
     // on-chip staging up to what the block's shared memory holds beside the
     // kernel's static arrays (each unit then keeps its slot rows on chip
     // when they fit beside its own lines)
@@ -1497,31 +1499,71 @@ int marfa_autotune(marfa_ctx *ctx, const marfa_run *run, int n_levels, const dou
   const Tune keep = ctx->tune;
   Tune best = keep;
   double best_ms = 1e300;
+  // one candidate: the best of two timed calls (the first call also grows buffers)
+  auto trial = [&](double &ms) -> int {
+    ms = 1e300;
+    for (int rep = 0; rep < 3; ++rep) {
+      Outputs o;
+      o.dev_out = (float *)ctx->b_tune.p;
+      int rc = run_levels(ctx, run, L, P.data(), T.data(), n.data(), o, ctx->stream);
+      if (!rc) rc = marfa_synchronize(ctx);
+      if (rc) return rc;
+      double t[8];
+      if (rep > 0 && marfa_last_timings(ctx, t) == MARFA_OK) ms = std::min(ms, t[5]);
+    }
+    return MARFA_OK;
+  };
   for (int fcv : {2048, 4096, 8192, 16384})
     for (int ck : {1, 2, 3, 4, 5}) {
       ctx->tune.far_chunk = fcv;
       ctx->tune.coop_k = ck;
-      double ms = 1e300;
-      for (int rep = 0; rep < 3; ++rep) { // the first call also grows buffers
-        Outputs o;
-        o.dev_out = (float *)ctx->b_tune.p;
-        int rc = run_levels(ctx, run, L, P.data(), T.data(), n.data(), o, ctx->stream);
-        if (!rc) rc = marfa_synchronize(ctx);
-        if (rc) {
-          ctx->tune = keep;
-          return rc;
-        }
-        double t[8];
-        if (rep > 0 && marfa_last_timings(ctx, t) == MARFA_OK) ms = std::min(ms, t[5]);
+      double ms;
+      if (int rc = trial(ms)) {
+        ctx->tune = keep;
+        return rc;
       }
       if (ms < best_ms) {
         best_ms = ms;
         best = ctx->tune;
       }
     }
+  // FP32c: the other fine-block shape at the best of the others
+  if (run->precision != MARFA_PREC_FP64) {
+    ctx->tune = best;
+    ctx->tune.fine_pair = !best.fine_pair;
+    double ms;
+    if (int rc = trial(ms)) {
+      ctx->tune = keep;
+      return rc;
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = ctx->tune;
+    }
+  }
   ctx->tune = best;
   if (far_chunk) *far_chunk = best.far_chunk;
   if (coop_k) *coop_k = best.coop_k;
+  return MARFA_OK;
+}
+
+int marfa_ctx_set_launch(marfa_ctx *ctx, int far_chunk, int coop_k, int fine_pair) {
+  if (!ctx) return MARFA_E_ARG;
+  if (far_chunk != 2048 && far_chunk != 4096 && far_chunk != 8192 && far_chunk != 16384)
+    return set_err(ctx, MARFA_E_ARG, "far_chunk %d (2048, 4096, 8192 or 16384)", far_chunk);
+  if (coop_k < 1 || coop_k > 5) return set_err(ctx, MARFA_E_ARG, "coop_k %d (1..5)", coop_k);
+  if (fine_pair != 0 && fine_pair != 1) return set_err(ctx, MARFA_E_ARG, "fine_pair %d (0 or 1)", fine_pair);
+  ctx->tune.far_chunk = far_chunk;
+  ctx->tune.coop_k = coop_k;
+  ctx->tune.fine_pair = fine_pair;
+  return MARFA_OK;
+}
+
+int marfa_ctx_get_launch(marfa_ctx *ctx, int *far_chunk, int *coop_k, int *fine_pair) {
+  if (!ctx) return MARFA_E_ARG;
+  if (far_chunk) *far_chunk = ctx->tune.far_chunk;
+  if (coop_k) *coop_k = ctx->tune.coop_k;
+  if (fine_pair) *fine_pair = ctx->tune.fine_pair;
   return MARFA_OK;
 }
 

@@ -744,6 +744,13 @@ __device__ __forceinline__ void grid0_line(const NearStore<F64> &st, int q, Lane
 // depend only on the parity of its bin (see pair_cells).
 // threads per block: 1024 in the FP32 form (64 registers), 512 in FP64
 __host__ __device__ constexpr int fine_threads(bool f64) { return f64 ? 512 : 1024; }
+// Resident blocks per SM each launch shape is compiled for: 256-thread blocks
+// four per SM, 512-thread FP32c blocks two per SM (the paired shape), the
+// widest blocks (1024 threads FP32c, 512 FP64) one per SM.  Every shape has
+// 64 registers per thread, except the FP64 one with 128.
+__host__ __device__ constexpr int fine_min_blocks(bool f64, int th) {
+  return th == 256 ? 4 : (!f64 && th == 512 ? 2 : 1);
+}
 __device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 
 // Line shape of one near line for the fine passes: region 0 inline, Kuntz
@@ -1340,7 +1347,7 @@ __device__ void fine_unit(const FineParams &p, int ub, unsigned char *fine_smem)
 // Persistent: every block takes units from the work queue until it is empty
 // (units in the given order, most near lines first).
 template <bool F64, int CHI, int TH>
-__global__ void __launch_bounds__(TH, TH == 256 ? 4 : 1) fine_kernel(FineParams p) {
+__global__ void __launch_bounds__(TH, fine_min_blocks(F64, TH)) fine_kernel(FineParams p) {
   extern __shared__ __align__(16) unsigned char fine_smem[];
   __shared__ int s_unit;
   for (;;) {
@@ -1639,8 +1646,34 @@ cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t 
 // Block size: fine_threads(F64) threads for dense units (the passes have
 // many sites and lines), SMALL_TH for workloads whose units have few near
 // lines: those are latency bound per unit, and small blocks put several
-// units on every SM.
+// units on every SM.  FP32c dense units can also run on PAIR_TH threads, two
+// blocks per SM, so that one block's barrier waits overlap the other's work.
 constexpr int SMALL_TH = 256;
+constexpr int PAIR_TH = 512;
+
+// Dynamic shared memory one block of a launch shape may take: the opt-in
+// limit per block minus the kernel's static arrays, and for the paired shape
+// its half of the SM's shared memory (less the static arrays and the
+// per-block reservation), rounded down to 1 KB.
+template <bool F64, int CHI, int TH>
+static cudaError_t fine_block_room(size_t *room) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI, TH>);
+  if (e != cudaSuccess) return e;
+  int dev = 0, optin = 0, per_sm = 0, reserved = 0;
+  if ((e = cudaGetDevice(&dev))) return e;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+  if ((e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev))) return e;
+  if ((e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev))) return e;
+  size_t r = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  constexpr int mb = fine_min_blocks(F64, TH);
+  if (TH != SMALL_TH && mb > 1) {
+    const size_t share = (size_t)per_sm / mb, fixed = fa.sharedSizeBytes + (size_t)reserved;
+    r = std::min(r, share > fixed ? (share - fixed) / 1024 * 1024 : (size_t)0);
+  }
+  *room = r;
+  return cudaSuccess;
+}
 
 template <bool F64, int CHI, int TH>
 static cudaError_t fine_launch_th(const FineParams &p, cudaStream_t st) {
@@ -1653,24 +1686,25 @@ static cudaError_t fine_launch_th(const FineParams &p, cudaStream_t st) {
 
 template <bool F64, int CHI>
 static cudaError_t fine_launch(const FineParams &p, cudaStream_t st) {
-  return p.block_threads == SMALL_TH ? fine_launch_th<F64, CHI, SMALL_TH>(p, st)
-                                     : fine_launch_th<F64, CHI, fine_threads(F64)>(p, st);
+  switch (p.block_threads) {
+  case SMALL_TH: return fine_launch_th<F64, CHI, SMALL_TH>(p, st);
+  case PAIR_TH: return fine_launch_th<F64, CHI, PAIR_TH>(p, st);
+  default: return fine_launch_th<F64, CHI, fine_threads(F64)>(p, st);
+  }
 }
 
-// Shared-memory plan of the fine kernel: large blocks (one per SM) take the
-// whole room a block may have and place each unit's slot rows there when
-// they fit; small blocks stage `smem_cap` lines, with slot rows when those
-// fit too.  Also the resident blocks of the persistent grid.
+// Shared-memory plan of the fine kernel: large blocks take the whole room a
+// block of their shape may have (fine_block_room) and place each unit's slot
+// rows there when they fit; small blocks stage `smem_cap` lines, with slot
+// rows when those fit too.  Also the resident blocks of the persistent grid.
 template <bool F64, int CHI, int TH>
 static cudaError_t fine_occupancy_th(int smem_cap, size_t *smem_room, int *blocks) {
-  cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI, TH>);
-  if (e != cudaSuccess) return e;
-  int dev = 0, sms = 0, optin = 0;
+  cudaError_t e;
+  int dev = 0, sms = 0;
   if ((e = cudaGetDevice(&dev))) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
-  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
-  const size_t room = (size_t)optin - fa.sharedSizeBytes;
+  size_t room = 0;
+  if ((e = fine_block_room<F64, CHI, TH>(&room))) return e;
   size_t smem = room;
   if (TH == SMALL_TH)
     smem = fine_smem_bytes(smem_cap, F64, fine_smem_bytes(smem_cap, F64, NSLOT) <= room ? NSLOT : 0);
@@ -1684,31 +1718,33 @@ static cudaError_t fine_occupancy_th(int smem_cap, size_t *smem_room, int *block
   return cudaSuccess;
 }
 
-// Most near lines one block stages in shared memory: the opt-in limit per
-// block minus the kernel's static shared memory, over the bytes per line.
+// Most near lines one block stages in shared memory: the room of a block of
+// this shape (fine_block_room) over the bytes per line.
 template <bool F64, int CHI, int TH>
 static cudaError_t fine_stage_limit_th(int *lines) {
-  cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, fine_kernel<F64, CHI, TH>);
+  size_t room = 0;
+  const cudaError_t e = fine_block_room<F64, CHI, TH>(&room);
   if (e != cudaSuccess) return e;
-  int dev = 0, optin = 0;
-  if ((e = cudaGetDevice(&dev))) return e;
-  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
-  const size_t room = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
   *lines = (int)(room / fine_smem_bytes(1, F64, 0)) / 128 * 128;
   return cudaSuccess;
 }
 
 template <bool F64, int CHI>
 static cudaError_t fine_stage_limit(int threads, int *lines) {
-  return threads == SMALL_TH ? fine_stage_limit_th<F64, CHI, SMALL_TH>(lines)
-                             : fine_stage_limit_th<F64, CHI, fine_threads(F64)>(lines);
+  switch (threads) {
+  case SMALL_TH: return fine_stage_limit_th<F64, CHI, SMALL_TH>(lines);
+  case PAIR_TH: return fine_stage_limit_th<F64, CHI, PAIR_TH>(lines);
+  default: return fine_stage_limit_th<F64, CHI, fine_threads(F64)>(lines);
+  }
 }
 
 template <bool F64, int CHI>
 static cudaError_t fine_occupancy(int threads, int smem_cap, size_t *room, int *blocks) {
-  return threads == SMALL_TH ? fine_occupancy_th<F64, CHI, SMALL_TH>(smem_cap, room, blocks)
-                             : fine_occupancy_th<F64, CHI, fine_threads(F64)>(smem_cap, room, blocks);
+  switch (threads) {
+  case SMALL_TH: return fine_occupancy_th<F64, CHI, SMALL_TH>(smem_cap, room, blocks);
+  case PAIR_TH: return fine_occupancy_th<F64, CHI, PAIR_TH>(smem_cap, room, blocks);
+  default: return fine_occupancy_th<F64, CHI, fine_threads(F64)>(smem_cap, room, blocks);
+  }
 }
 
 template <bool F64>
@@ -1737,8 +1773,9 @@ size_t fine_smem_bytes(int cap, bool f64, int rows) {
 }
 size_t fine_vbuf_elems(int cap) { return (size_t)NSLOT * cap; }
 
-int fine_block_threads(int precision, int max_near, int small_below) {
-  return max_near < small_below ? SMALL_TH : fine_threads(precision == 0);
+int fine_block_threads(int precision, int max_near, int small_below, int pair) {
+  if (max_near < small_below) return SMALL_TH;
+  return precision != 0 && pair ? PAIR_TH : fine_threads(precision == 0);
 }
 
 cudaError_t fine_smem_lines(int precision, int chi, int threads, int *lines) {

@@ -202,8 +202,9 @@ cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st)
 size_t fine_smem_bytes(int cap, bool f64, int rows = 0);
 size_t fine_vbuf_elems(int cap);
 // block size of the fine kernel for a batch whose units have at most
-// `max_near` near lines (small blocks below `small_below` lines)
-int fine_block_threads(int precision, int max_near, int small_below);
+// `max_near` near lines (small blocks below `small_below` lines; pair != 0:
+// FP32c dense units on two 512-thread blocks per SM instead of one of 1024)
+int fine_block_threads(int precision, int max_near, int small_below, int pair);
 // most near lines a block of `threads` stages in shared memory (the opt-in
 // limit minus the kernel's static shared memory)
 cudaError_t fine_smem_lines(int precision, int chi, int threads, int *lines);

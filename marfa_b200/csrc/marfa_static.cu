@@ -334,7 +334,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
         !ck(cudaStreamSynchronize(st), "sync near"))
       return rc;
   }
-  fn.block_threads = fine_block_threads(run->precision, 1 << 30, 0);
+  fn.block_threads = fine_block_threads(run->precision, 1 << 30, 0, 0);
   int smem_lines = 0;
   if (!ck(fine_smem_lines(run->precision, chi, fn.block_threads, &smem_lines), "fine shared memory")) return rc;
   const int smem_max = std::min(f64 ? 4096 : 2816, smem_lines);
