@@ -190,7 +190,7 @@ void marfa_graph_destroy(marfa_graph *graph);
 /* Chooses the context's launch parameters that do not change the method --
  * lines per far-kernel block (far_chunk: 2048, 4096, 8192 or 16384) and the number of
  * coarse fine grids whose accumulators are summed by groups of lanes rather
- * than one thread each (coop_k: 1..5) -- by timing every candidate on up to four levels of the given
+ * than one thread each (coop_k: 1..5) -- by timing every candidate on up to sixteen levels of the given
  * profile; for FP32c it then times the other fine-kernel block shape
  * (fine_pair, see marfa_ctx_set_launch) at the best of those.  Keeps the
  * fastest in the context and returns far_chunk and coop_k (the shape through

@@ -1481,10 +1481,14 @@ int marfa_autotune(marfa_ctx *ctx, const marfa_run *run, int n_levels, const dou
   if (!run || n_levels < 1 || !pressure || !temperature || !density)
     return set_err(ctx, MARFA_E_ARG, "null argument");
   if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MARFA_E_CUDA, "cudaSetDevice");
-  // sample: up to four levels spread over the profile, every subinterval
+  // sample: up to sixteen levels spread over the profile, every subinterval
+  // (a far-kernel grid of a few levels has too few blocks and favours small
+  // chunks that lose on a whole profile)
+  constexpr int kSample = 16;
   std::vector<int> pick;
-  for (int j = 0; j < std::min(4, n_levels); ++j) {
-    const int l = n_levels == 1 ? 0 : (int)std::lround((double)j * (n_levels - 1) / (std::min(4, n_levels) - 1));
+  for (int j = 0; j < std::min(kSample, n_levels); ++j) {
+    const int l = n_levels == 1 ? 0
+                                : (int)std::lround((double)j * (n_levels - 1) / (std::min(kSample, n_levels) - 1));
     if (pick.empty() || pick.back() != l) pick.push_back(l);
   }
   std::vector<double> P, T, n;
