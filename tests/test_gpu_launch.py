@@ -4,11 +4,13 @@ outside the tuned sets are refused, and the FP32c fine-kernel block shapes
 results: within 1e-5 of the FP64 oracle where k > 1e-6 max(k) (outside
 cascade near-ties), on a workload whose densest units stage in global
 memory under the paired shape.  FP64 ignores the shape (bit-identical
-records)."""
+records), and every far-kernel chunk size and lane-group setting keeps the
+FP64 records within 1e-12 of the oracle."""
 import numpy as np
 import pytest
 
 import oracle as O
+from conftest import rel_err
 from fp32c_check import check_fp32c
 from marfa_b200 import synth
 from marfa_b200._lib import MarfaError
@@ -60,3 +62,23 @@ def test_fine_block_shapes_match_oracle(gpu, tips):
         print(f"fine_pair={pair}: max err {e32:.3e} outside {taint} near-tie points")
         assert e32 <= 1e-5 and taint <= 1e-4 * ref.size
     assert np.array_equal(r64[0], r64[1])
+
+
+@pytest.mark.parametrize("far_chunk,coop_k", [(2048, 1), (4096, 3), (8192, 5), (16384, 2)])
+def test_launch_parameters_keep_fp64_parity(gpu, tips, far_chunk, coop_k):
+    """Every far-kernel chunk size (the cp.async tiles then end inside a
+    tile at many chunk boundaries) and lane-group setting gives FP64 records
+    within 1e-12 of the all-double oracle."""
+    w = synth.config(1, scale=0.03)
+    p = w.profiles[0]
+    lv = slice(0, 40, 13)
+    P, T, n = p.pressure[lv], p.temperature[lv], p.density[lv]
+    orc = O.Oracle(w.lines, tips, P, T, n, w.start_wv, w.end_wv, w.cutoff, target=w.target, chi=w.chi,
+                   precision=O.FP64)
+    _, ref, _ = orc.run()
+    with Context(w.lines, tips) as ctx:
+        ctx.set_launch(far_chunk, coop_k, 0)
+        _, g64 = ctx.compute(Run(w.start_wv, w.end_wv, w.cutoff, target=w.target, molecule=w.molecule,
+                                 chi=w.chi, precision="fp64"), P, T, n, want64=True)
+    err, npts = rel_err(g64, ref, 0.0)
+    assert npts == ref.size and err <= 1e-12, err
