@@ -44,7 +44,7 @@ FLOP_PER_EVAL = 12  # chi-corrected Lorentz evaluation + accumulation, FMA = 2
 CASCADE_BYTES_PER_RECORD = 10230 * 3 * 4 + 20481 * 4
 # fine kernel DRAM traffic per unit (one level x subinterval), from one ncu
 # capture of the two-level Venus case scaled by its units
-FINE_TRAFFIC_PER_UNIT = 257_164  # (31,557,120 + 19,875,584) B / 200 units
+FINE_TRAFFIC_PER_UNIT = 259_657  # (31,573,248 + 20,358,144) B / 200 units
 FINE_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one fine_kernel launch "
                        "on levels 1 and 21 (200 units), scaled by units: "
                        "profiles/fine_kernel_fp32c_venus_2levels.md")
