@@ -10,7 +10,10 @@ across subinterval edges) to the top of the profile, for both targets:
 - line windows equal to the oracle's;
 - evaluation counts equal to the oracle's;
 - FP64 records within 1e-12 of the all-double oracle on every point;
-- FP32c within 1e-5 where k > 1e-6 max(k), outside cascade near-ties."""
+- FP32c within 1e-5 where k > 1e-6 max(k), outside cascade near-ties.
+And the `marfa` command run on the same files in the reference's directory
+layout writes PT files equal to the oracle's records within float32
+rounding at every level of the profile."""
 from pathlib import Path
 
 import numpy as np
@@ -57,3 +60,45 @@ def test_real_co_band_matches_oracle(gpu, tips, real, target):
     print(f"{target}: {int(ev_ref.sum())} evaluations, FP64 max err {err:.2e}, "
           f"FP32c max err {e32:.2e} outside {taint} near-tie points")
     assert e32 <= 1e-5 and taint <= 1e-4 * ref.size
+
+
+def test_marfa_command_on_reference_inputs(gpu, tips, tmp_path):
+    """`marfa CO 2000 2100 HITRAN2020 25 VAC VenusCO2-3.dat fp64` in a tree of
+    the reference's layout (its CO line slice as data/databases/HITRAN2020.05,
+    its profile, the TIPS rows in the full-table layout) writes one PT file
+    per level of the 66-level profile; every record equals the all-double
+    oracle's within float32 rounding (1e-6)."""
+    import subprocess
+    from marfa_b200 import build, data_path
+    from marfa_b200.io import RECORD_BYTES, pt_name, record_number, subinterval_starts
+    for d in ("data/Atmospheres", "data/databases", "data/TIPS", "output/ptTables"):
+        (tmp_path / d).mkdir(parents=True)
+    (tmp_path / "data/databases/HITRAN2020.05").write_bytes((GOLD / "co_hitran2020_1900_2400.lines").read_bytes())
+    (tmp_path / "data/Atmospheres/VenusCO2-3.dat").write_bytes((GOLD / "VenusCO2-3.dat").read_bytes())
+    sub = data_path("TIPS_subset.dat").read_text().splitlines()
+    rows = {int(l.split(":")[0]): l.split(":", 1)[1].strip() for l in sub[1:]}
+    zero = ", ".join(["0.0"] * 501)
+    (tmp_path / "data/TIPS/TIPS.dat").write_text(
+        "74, 501\n" + "\n".join(rows.get(i, zero) for i in range(1, 75)) + "\n")
+    build.build()
+    marfa = Path(__file__).resolve().parent.parent / "marfa_b200" / "marfa"
+    r = subprocess.run([str(marfa), "CO", "2000", "2100", "HITRAN2020", "25", "VAC", "VenusCO2-3.dat", "fp64"],
+                       cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    latest = (tmp_path / "output/ptTables/latest_run.txt").read_text().strip()
+    out = tmp_path / "output/ptTables" / latest
+    lines = read_lines(GOLD / "co_hitran2020_1900_2400.lines")
+    _, _, P, T, n = read_profile(GOLD / "VenusCO2-3.dat")
+    orc = O.Oracle(lines, tips, P, T, n, 2000.0, 2100.0, 25.0, target="VAC", chi="none", mol_code=5,
+                   precision=O.FP64)
+    _, ref, _ = orc.run()
+    starts = subinterval_starts(2000.0, 2100.0)
+    worst = 0.0
+    for lev in range(len(P)):
+        raw = (out / pt_name(lev + 1)).read_bytes()
+        for i, s in enumerate(starts):
+            k = record_number(s) - 1
+            rec = np.frombuffer(raw[k * RECORD_BYTES:(k + 1) * RECORD_BYTES], dtype="<f4")
+            worst = max(worst, rel_err(rec, ref[lev, i], 0.0)[0])
+    print(f"{len(P)} levels x {len(starts)} records: max err {worst:.2e}")
+    assert worst <= 1e-6
