@@ -114,12 +114,57 @@ __device__ __forceinline__ int64_t upper_bound_d(const double *a, int64_t n, dou
   return lo;
 }
 
+// Lines of the block's re-ordering window that fit in shared memory: the
+// block's 256 lines and the lines within the level's margin of them (at the
+// densest Venus levels about 1,000).
+constexpr int RANK_TILE = 2048;
+
+// The block's lines share one window [w0, w1) of unshifted centres (every
+// line's own window lies inside it, as the centres are sorted): when it fits,
+// the centres and shifted keys of the window are staged in shared memory once
+// and every thread's searches and comparisons run there; otherwise each
+// thread searches and scans the global arrays.  Both give the same rank.
 __global__ void __launch_bounds__(256) rank_kernel(SortParams p) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double s_nu[RANK_TILE], s_key[RANK_TILE];
+  __shared__ int64_t s_w[2];
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x, i = i0 + threadIdx.x;
   const int l = blockIdx.y;
-  if (i >= p.n) return;
+  const int64_t i1 = min(i0 + (int64_t)blockDim.x, p.n); // the block's lines [i0, i1)
   const double *key = p.nus + (size_t)l * p.n;
   const double m = p.margin[l];
+  if (threadIdx.x == 0) s_w[0] = lower_bound_d(p.nu, p.n, p.nu[i0] - m);
+  if (threadIdx.x == 32) s_w[1] = upper_bound_d(p.nu, p.n, p.nu[i1 - 1] + m);
+  __syncthreads();
+  const int64_t w0 = s_w[0], w1 = s_w[1];
+  if (w1 - w0 <= RANK_TILE) {
+    const int w = (int)(w1 - w0);
+    for (int j = threadIdx.x; j < w; j += blockDim.x) {
+      s_nu[j] = p.nu[w0 + j];
+      s_key[j] = key[w0 + j];
+    }
+    __syncthreads();
+    if (i >= p.n) return;
+    const int t = (int)(i - w0);
+    const double nu = s_nu[t], k = s_key[t];
+    int a = 0, b = w; // first window entry with centre >= nu - m
+    while (a < b) {
+      const int c = (a + b) >> 1;
+      if (s_nu[c] < nu - m) a = c + 1; else b = c;
+    }
+    int e = a, f = w; // first entry with centre > nu + m
+    while (e < f) {
+      const int c = (e + f) >> 1;
+      if (s_nu[c] <= nu + m) e = c + 1; else f = c;
+    }
+    int64_t r = w0 + a;
+    for (int j = a; j < e; ++j) {
+      const double kj = s_key[j];
+      r += (kj < k) || (kj == k && j < t);
+    }
+    p.rank[(size_t)l * p.n + i] = r;
+    return;
+  }
+  if (i >= p.n) return;
   const double nu = p.nu[i], k = key[i];
   const int64_t jlo = lower_bound_d(p.nu, p.n, nu - m);
   const int64_t jhi = upper_bound_d(p.nu, p.n, nu + m);
