@@ -8,7 +8,8 @@
   edges: the window exit uses the unshifted centre (LBL.f90:57), the
   placement the shifted one (LBL.f90:81-98, Spectroscopy.f90:38-49);
 * a dense band of 5,000 lines within one subinterval and 1 cm-1 around it
-  (more near lines than the fine kernel stages on chip);
+  (more near lines than the fine kernel stages on chip), and a shifted band
+  whose re-ordering windows exceed the rank kernel's shared-memory tile;
 * the full Venus workload (200,000 lines, 40 levels x 100 subintervals).
 
 Tolerances: FP64 1e-12 relative on every point against the all-double
@@ -123,6 +124,21 @@ def dense_band(n=5000, seed=31):
 def test_dense_band_beyond_on_chip_staging(gpu, tips):
     lines = dense_band()
     prof = profile([1.0, 0.01], [296.0, 250.0])
+    with Context(lines, tips) as ctx:
+        check_all(ctx, lines, tips, prof, START, END, 25.0, placement_subs=(1,))
+
+
+def test_reordering_window_beyond_the_rank_tile(gpu, tips):
+    """12,000 lines over 20 cm-1 (600 per cm-1) with delta in [-0.01, 0.01]:
+    at 92 atm a block's re-ordering window holds about 2,500 lines (more than
+    the 2,048 the rank kernel stages in shared memory: the global path), at
+    20 atm about 750 (the shared-memory path); records match the oracle at
+    both levels."""
+    lines = synth.make_lines(synth.LineSpec(n=12_000, nu_lo=4045.0, nu_hi=4065.0,
+                                            delta=(-0.01, 0.01), seed=33))
+    per_cm = 12_000 / 20.0
+    assert 256 + 2 * per_cm * 0.02 * 92.0 > 2048 > 256 + 2 * per_cm * 0.02 * 20.0
+    prof = profile([92.0, 20.0], [735.0, 650.0])
     with Context(lines, tips) as ctx:
         check_all(ctx, lines, tips, prof, START, END, 25.0, placement_subs=(1,))
 
