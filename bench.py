@@ -274,7 +274,7 @@ def run_b200(args, rank, world, local_rank):
     clk = clocks.stop()
     barrier()
     # FP64 drop-in
-    ms64, tm64, _ = timed_steps(ctx, run64, [L], P, T, n, out64, stream, max(2, args.steps // 2), args.warmup)
+    ms64, tm64, _ = timed_steps(ctx, run64, [L], P, T, n, out64, stream, args.steps, args.warmup)
     barrier()
     from marfa_b200.multi import reduce_step
     ms_max, total_evals = reduce_step(ms32, evals, dist)  # slowest rank, work of all ranks
