@@ -45,6 +45,9 @@ CASCADE_BYTES_PER_RECORD = 10230 * 3 * 4 + 20481 * 4
 # fine kernel DRAM traffic per unit (one level x subinterval), from one ncu
 # capture of the two-level Venus case scaled by its units
 FINE_TRAFFIC_PER_UNIT = 259_657  # (31,573,248 + 20,358,144) B / 200 units
+# fine kernel warp instructions per unit, from the same capture: the kernel
+# is issue-bound, so its issue rate is the roofline that describes it
+FINE_WARP_INST_PER_UNIT = 755_935  # 151,187,000 warp instructions / 200 units
 FINE_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one fine_kernel launch "
                        "on levels 1 and 21 (200 units), scaled by units: "
                        "profiles/fine_kernel_fp32c_venus_2levels.md")
@@ -320,6 +323,17 @@ def run_b200(args, rank, world, local_rank):
                             if dom == "fine" and FINE_TRAFFIC_PER_UNIT else None),
                 "traffic_source": FINE_TRAFFIC_SOURCE if dom == "fine" else None}
     far_roof = FLOP_PER_EVAL * far_evals / (tm32["far"] * 1e-3) / 1e12
+    # issue roofline of the fine kernel: warp instructions per second against
+    # one instruction per scheduler per clock (4 per SM) at the sampled clock
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    sm_mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    issue_peak = sms * 4 * sm_mhz * 1e6
+    issue = FINE_WARP_INST_PER_UNIT * L * run32.n_sub / (tm32["fine"] * 1e-3)
+    fine_issue = {"kernel": "fine_kernel (fp32c)", "achieved": issue / 1e12, "peak": issue_peak / 1e12,
+                  "unit": "T warp-instructions/s", "frac": issue / issue_peak,
+                  "peak_source": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz (sampled)",
+                  "inst_source": "ncu smsp__inst_executed.sum of the capture in "
+                                 "profiles/fine_kernel_fp32c_venus_2levels.md, per unit"}
     hbm, hbm_src = hbm_peak()
     records = L * run32.n_sub
     cascade_gbs = records * CASCADE_BYTES_PER_RECORD / (tm32["cascade"] * 1e-3) / 1e9
@@ -363,6 +377,7 @@ def run_b200(args, rank, world, local_rank):
             "kernel_ms_fp64": {k: round(tm64[k], 4) for k in fams},
             "roofline": roof,
             "far_kernel_tflops": far_roof,
+            "fine_issue_roofline": fine_issue,
             "fma_peak_tflops": {"fp32": fp32_peak[0] / 1e12, "fp64": fp64_peak[0] / 1e12},
             "cascade_hbm": {"achieved_gbs": cascade_gbs, "peak_gbs": hbm, "frac": cascade_gbs / hbm,
                             "peak_source": hbm_src,
