@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(256) cascade_adjoint_kernel(CascadeAdjParams p
   __shared__ double gv[1023 * 3];  // their gradients
   if (threadIdx.x < 32) { // grid-0 cell J as cascade_kernel forms it
     double f[4];
-    far_cell_sums(p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
+    far_sums(p.fold ? p.fold + ((size_t)l * p.n_sub + sub) * NFAR : nullptr,
+             p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
     if (threadIdx.x == 0) {
       val[0] = f[0] + scr[1 + J - 1];
       val[1] = f[1] + scr[11 + J - 1];

@@ -113,9 +113,9 @@ struct marfa_ctx {
   double *d_tips = nullptr;
   int *d_err = nullptr;
   // grow-only work buffers
-  DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_scr, b_lv, b_margin, b_win, b_chunks,
+  DevBuf b_nus, b_gen, b_hot, b_rank, b_snu, b_sidx, b_far, b_fold, b_scr, b_lv, b_margin, b_win, b_chunks,
       b_out, b_out64, b_dump, b_count, b_gstage, b_aux, b_gscr, b_cot, b_grad, b_vbuf, b_queue, b_order, b_tune;
-  DevBuf b2_nus, b2_gen, b2_hot, b2_rank, b2_snu, b2_sidx, b2_far, b2_scr, b2_gstage, b2_vbuf, b2_queue;
+  DevBuf b2_nus, b2_gen, b2_hot, b2_rank, b2_snu, b2_sidx, b2_far, b2_fold, b2_scr, b2_gstage, b2_vbuf, b2_queue;
   std::string err;
   // pinned staging of the per-call host tables (see Staging): a ring of
   // buffers, used by consecutive calls in turn
@@ -495,14 +495,14 @@ struct Timeline {
 
 // The per-chunk device buffers: set 1 is the second stream's copy.
 struct ChunkBufs {
-  DevBuf *nus, *gen, *hot, *rank, *snu, *sidx, *far, *scr, *gstage, *vbuf, *queue;
+  DevBuf *nus, *gen, *hot, *rank, *snu, *sidx, *far, *fold, *scr, *gstage, *vbuf, *queue;
 };
 static ChunkBufs chunk_bufs(marfa_ctx *ctx, int set) {
   if (set)
     return {&ctx->b2_nus, &ctx->b2_gen, &ctx->b2_hot, &ctx->b2_rank, &ctx->b2_snu, &ctx->b2_sidx, &ctx->b2_far,
-            &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue};
-  return {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far, &ctx->b_scr,
-          &ctx->b_gstage, &ctx->b_vbuf, &ctx->b_queue};
+            &ctx->b2_fold, &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue};
+  return {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far, &ctx->b_fold,
+          &ctx->b_scr, &ctx->b_gstage, &ctx->b_vbuf, &ctx->b_queue};
 }
 
 // Precision constants, the memory plan (levels per chunk, units per batch)
@@ -608,6 +608,7 @@ static int alloc_buffers(marfa_ctx *ctx, int n_levels, const double *P, const Ou
   CK(ensure(ctx, ctx->b_snu, (size_t)Lc * N * 8), "alloc snu");
   CK(ensure(ctx, ctx->b_sidx, (size_t)Lc * N * 4), "alloc sidx");
   CK(ensure(ctx, ctx->b_far, (size_t)Lc * std::max(C, 1) * NFAR * 8), "alloc far");
+  CK(ensure(ctx, ctx->b_fold, (size_t)Lc * nsub * NFAR * 8), "alloc far sums");
   CK(ensure(ctx, ctx->b_scr, (size_t)UB * SCR_STRIDE * elem), "alloc scratch");
   if (two) {
     CK(ensure(ctx, ctx->b2_nus, ctx->b_nus.cap), "alloc nus");
@@ -617,6 +618,7 @@ static int alloc_buffers(marfa_ctx *ctx, int n_levels, const double *P, const Ou
     CK(ensure(ctx, ctx->b2_snu, ctx->b_snu.cap), "alloc snu");
     CK(ensure(ctx, ctx->b2_sidx, ctx->b_sidx.cap), "alloc sidx");
     CK(ensure(ctx, ctx->b2_far, ctx->b_far.cap), "alloc far");
+    CK(ensure(ctx, ctx->b2_fold, ctx->b_fold.cap), "alloc far sums");
     CK(ensure(ctx, ctx->b2_scr, ctx->b_scr.cap), "alloc scratch");
   }
   if (adj) {
@@ -883,6 +885,10 @@ static int launch_chunk(marfa_ctx *ctx, const marfa_run *run, const Outputs &o, 
     ctx->far_launches += 1;
   }
   if (e3) cudaEventRecord(e3, cs);
+  // far sums per (level, subinterval, grid-0 position), read by the cascade
+  double *fold = (double *)B.fold->p;
+  CK(launch_far_fold(fp.out, d_sc0, C, nsub, nl, fold, cs), "far sums");
+  ctx->launches += 1;
   mark(0, e0, e1);
   mark(1, e1, e2);
   mark(2, e2, e3);
@@ -938,6 +944,7 @@ static int launch_chunk(marfa_ctx *ctx, const marfa_run *run, const Outputs &o, 
       CascadeAdjParams ca;
       ca.scratch = (const double *)B.scr->p;
       ca.far = fp.out;
+      ca.fold = fold;
       ca.sub_chunk0 = d_sc0;
       ca.lv = pp.lv;
       ca.n_chunks = C;
@@ -982,6 +989,7 @@ static int launch_chunk(marfa_ctx *ctx, const marfa_run *run, const Outputs &o, 
     CascadeParams cp;
     cp.scratch = B.scr->p;
     cp.far = fp.out;
+    cp.fold = fold;
     cp.sub_chunk0 = d_sc0;
     cp.lv = pp.lv;
     cp.n_chunks = C;
@@ -1253,12 +1261,12 @@ void marfa_ctx_destroy(marfa_ctx *ctx) {
                 ctx->d_iso, ctx->d_tips, ctx->d_err, ctx->d_S64, ctx->d_gair64};
   for (void *p : ps)
     if (p) cudaFree(p);
-  DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far,
+  DevBuf *bs[] = {&ctx->b_nus, &ctx->b_gen, &ctx->b_hot, &ctx->b_rank, &ctx->b_snu, &ctx->b_sidx, &ctx->b_far, &ctx->b_fold,
                   &ctx->b_scr, &ctx->b_lv, &ctx->b_margin, &ctx->b_win, &ctx->b_chunks, &ctx->b_out,
                   &ctx->b_out64, &ctx->b_dump, &ctx->b_count, &ctx->b_gstage, &ctx->b_aux,
                   &ctx->b_gscr, &ctx->b_cot, &ctx->b_grad, &ctx->b_vbuf, &ctx->b_queue, &ctx->b_order, &ctx->b_tune,
                   &ctx->b2_nus, &ctx->b2_gen, &ctx->b2_hot, &ctx->b2_rank, &ctx->b2_snu, &ctx->b2_sidx,
-                  &ctx->b2_far, &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue};
+                  &ctx->b2_far, &ctx->b2_fold, &ctx->b2_scr, &ctx->b2_gstage, &ctx->b2_vbuf, &ctx->b2_queue};
   for (DevBuf *b : bs) release(*b);
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);

@@ -435,4 +435,19 @@ __device__ __forceinline__ void far_cell_sums(const double *far, int c0, int c1,
     for (int i = 0; i < 4; ++i) f[i] += __shfl_xor_sync(0xffffffffu, f[i], off);
 }
 
+// Far-line sums of grid-0 cell J of one unit: read from the unit's folded
+// row (its far-kernel chunks summed per position by far_fold_kernel) when
+// there is one, else summed here over the chunks.
+__device__ __forceinline__ void far_sums(const double *fold, const double *far, int c0, int c1, int J,
+                                         double (&f)[4]) {
+  if (fold) {
+    f[0] = fold[2 * (J - 1)];
+    f[1] = fold[2 * J - 1];
+    f[2] = fold[2 * J];
+    f[3] = fold[0];
+  } else {
+    far_cell_sums(far, c0, c1, J, f);
+  }
+}
+
 } // namespace marfa

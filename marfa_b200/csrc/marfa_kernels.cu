@@ -1456,7 +1456,8 @@ __global__ void __launch_bounds__(256) cascade_kernel(CascadeParams p) {
   // grid-0 cell J: far-line sums (every warp reduces them itself, in the same
   // order) plus the near part
   double f[4];
-  far_cell_sums(p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
+  far_sums(p.fold ? p.fold + ((size_t)l * p.n_sub + sub) * NFAR : nullptr,
+           p.far + ((size_t)l * p.n_chunks) * NFAR, p.sub_chunk0[sub], p.sub_chunk0[sub + 1], J, f);
   double cP = (f[0] + (double)scr[1 + J - 1]) * inv;
   double cM = (f[1] + (double)scr[11 + J - 1]) * inv;
   double cL = (f[2] + (double)scr[21 + J - 1]) * inv;
@@ -1517,6 +1518,22 @@ __global__ void __launch_bounds__(256) cascade_kernel(CascadeParams p) {
   }
   const int tail0 = head + 4 * nvec;
   if ((int)threadIdx.x < 2048 - tail0) dst[tail0 + threadIdx.x] = outb[tail0 + threadIdx.x];
+}
+
+// Far-line sums of every (level, subinterval, grid-0 position) over the
+// subinterval's far-kernel chunks, in chunk order (one thread each), so that
+// the cascade reads its cells' far sums directly.
+__global__ void __launch_bounds__(256) far_fold_kernel(const double *far, const int *sub_chunk0, int n_chunks,
+                                                       int n_sub, int n_levels, double *fold) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n_levels * n_sub * NFAR) return;
+  const int e = (int)(idx % NFAR);
+  const int64_t ls = idx / NFAR;
+  const int sub = (int)(ls % n_sub), l = (int)(ls / n_sub);
+  const double *fl = far + (size_t)l * n_chunks * NFAR;
+  double s = 0.0;
+  for (int c = sub_chunk0[sub]; c < sub_chunk0[sub + 1]; ++c) s += fl[(size_t)c * NFAR + e];
+  fold[idx] = s;
 }
 
 // Raw accumulators of one unit in the oracle's layout (diagnostics).
@@ -1846,6 +1863,14 @@ cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_
 cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st) {
   if (p.n_units == 0) return cudaSuccess;
   near_count_kernel<<<(p.n_units + 255) / 256, 256, 0, st>>>(p, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_far_fold(const double *far, const int *sub_chunk0, int n_chunks, int n_sub, int n_levels,
+                            double *fold, cudaStream_t st) {
+  const int64_t n = (int64_t)n_levels * n_sub * NFAR;
+  if (n == 0) return cudaSuccess;
+  far_fold_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(far, sub_chunk0, n_chunks, n_sub, n_levels, fold);
   return cudaGetLastError();
 }
 

@@ -106,6 +106,7 @@ struct FineParams {
 struct CascadeParams {
   const void *scratch;           // from the fine kernel
   const double *far;             // [Lc][C][NFAR]
+  const double *fold;            // [Lc][n_sub][NFAR] far sums per unit, or null (summed from far)
   const int *sub_chunk0;         // [n_sub + 1] first chunk of each subinterval
   const LevelConst *lv;
   int n_chunks, n_sub;
@@ -155,6 +156,7 @@ struct AdjPrepParams {
 struct CascadeAdjParams {
   const double *scratch;         // FP64 accumulators of the batch
   const double *far;             // [Lc][C][NFAR]
+  const double *fold;            // [Lc][n_sub][NFAR] far sums per unit, or null
   const int *sub_chunk0;
   const LevelConst *lv;
   int n_chunks, n_sub;
@@ -195,6 +197,10 @@ cudaError_t launch_line_adjoint(const AdjointParams &p, int chi, int near_blocks
 cudaError_t launch_prep(const PrepParams &p, cudaStream_t st);
 cudaError_t launch_sort(const SortParams &p, cudaStream_t st);
 cudaError_t launch_far(const FarParams &p, int precision, int chi, cudaStream_t st);
+// far-kernel partials summed per (level, subinterval, grid-0 position) over
+// the subinterval's chunks, in chunk order: fold[Lc][n_sub][NFAR]
+cudaError_t launch_far_fold(const double *far, const int *sub_chunk0, int n_chunks, int n_sub, int n_levels,
+                            double *fold, cudaStream_t st);
 cudaError_t launch_fine(const FineParams &p, int precision, int chi, cudaStream_t st);
 cudaError_t launch_near_count(const FineParams &p, int *counts, cudaStream_t st);
 // shared memory of `cap` staged lines and `rows` slot-buffer rows of `cap`

@@ -361,6 +361,7 @@ extern "C" int marfa_compute_record_static(const marfa_line_record *lines, int64
   CascadeParams cp;
   cp.scratch = base + OFF_SCR;
   cp.far = fp.out;
+  cp.fold = nullptr; // one unit: summed from the chunks in the cascade
   cp.sub_chunk0 = d_small->sub_chunk0;
   cp.lv = pp.lv;
   cp.n_chunks = C;
