@@ -10,7 +10,10 @@
 //                   multigrid cell's contributing lines are one contiguous run.
 //   far_kernel      lines at least 1 cm-1 outside the subinterval: 21 grid-0
 //                   evaluations each, one thread per line, register sums,
-//                   block reduction (leftLBL / rightLBL grid-0 part).
+//                   block reduction (leftLBL / rightLBL grid-0 part); line
+//                   tiles staged through shared memory by cp.async.
+//   far_fold_kernel the far kernel's chunk partials summed per (level,
+//                   subinterval, grid-0 position) for the cascade.
 //   fine_kernel     lines within 1 cm-1 of / inside the subinterval: every
 //                   remaining accumulator (grid 0 near part, grids 1..9, direct
 //                   finest points) gathered per accumulator over its
