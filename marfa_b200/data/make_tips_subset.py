@@ -1,6 +1,7 @@
 """Extract the TIPS rows used by the workloads (isotopologue 1, H2O 161, and
-10, CO2 626, of the synthetic ones; 46-51, the six CO isotopologues of the
-real-data test) from a reference TIPS table into TIPS_subset.dat.
+10, CO2 626, of the synthetic ones; 46-51, the six CO isotopologues, and
+59-61, the three O2 isotopologues, of the real-data tests) from a reference
+TIPS table into TIPS_subset.dat.
 
 The partition sums are physical data (Gamache et al. 2017, as shipped in the
 reference's data/TIPS/TIPS.dat) that the intensity scaling must reproduce
@@ -11,7 +12,7 @@ reference tree is present:
 import sys
 from pathlib import Path
 
-ROWS = (1, 10, 46, 47, 48, 49, 50, 51)
+ROWS = (1, 10, 46, 47, 48, 49, 50, 51, 59, 60, 61)
 
 
 def main():

@@ -1,12 +1,14 @@
-"""GPU parity on the reference's own inputs: its CO line database (the
-1900-2400 cm-1 slice of data/databases/HITRAN2020.05: six isotopologues,
-HITRAN pressure shifts down to -0.019 cm-1/atm) and its Haus 2015 Venus
-profile (data/Atmospheres/VenusCO2-3.dat), as fixtures made by
-tests/golden/make_real_golden.py.
+"""GPU parity on the reference's own inputs: slices of its CO and O2 line
+databases (data/databases/HITRAN2020.05, 1900-2400 cm-1: six isotopologues,
+HITRAN pressure shifts down to -0.019 cm-1/atm; HITRAN2020.07, 12900-13300
+cm-1: the A band of three isotopologues, centres near 1.3e4 cm-1) and its
+Haus 2015 Venus profile (data/Atmospheres/VenusCO2-3.dat), as fixtures made
+by tests/golden/make_real_golden.py.
 
-Over 2000-2300 cm-1 with a 25 cm-1 cutoff, at six levels from the surface
-(91 atm, 733 K: shifts of up to -1.7 cm-1 reorder the lines and move them
-across subinterval edges) to the top of the profile, for both targets:
+Over 2000-2300 cm-1 (CO, both targets) and 13000-13200 cm-1 (O2) with a 25
+cm-1 cutoff, at six levels from the surface (91 atm, 733 K: shifts of up to
+-1.7 cm-1 reorder the lines and move them across subinterval edges) to the
+top of the profile:
 - line windows equal to the oracle's;
 - evaluation counts equal to the oracle's;
 - FP64 records within 1e-12 of the all-double oracle on every point;
@@ -28,27 +30,32 @@ from marfa_b200.io import read_lines, read_profile
 pytestmark = pytest.mark.gpu
 
 GOLD = Path(__file__).resolve().parent / "golden"
-START, END, CUT = 2000.0, 2300.0, 25.0
+CUT = 25.0
+# (fixture, molecule, HITRAN molecule number, interval): the CO fundamental
+# band and the O2 A band (centres near 1.3e4 cm-1, against grid offsets of
+# 5e-4 cm-1)
+BANDS = {"co": ("co_hitran2020_1900_2400.lines", "CO", 5, 2000.0, 2300.0),
+         "o2": ("o2_hitran2020_12900_13300.lines", "O2", 7, 13000.0, 13200.0)}
 
 
-@pytest.fixture(scope="module")
-def real():
-    lines = read_lines(GOLD / "co_hitran2020_1900_2400.lines")
+def levels():
     _, _, P, T, n = read_profile(GOLD / "VenusCO2-3.dat")
     lv = np.arange(0, len(P), 13)
-    return lines, P[lv], T[lv], n[lv]
+    return P[lv], T[lv], n[lv]
 
 
-@pytest.mark.parametrize("target", ["ACS", "VAC"])
-def test_real_co_band_matches_oracle(gpu, tips, real, target):
-    lines, P, T, n = real
-    orc = O.Oracle(lines, tips, P, T, n, START, END, CUT, target=target, chi="none", mol_code=5,
+@pytest.mark.parametrize("band,target", [("co", "ACS"), ("co", "VAC"), ("o2", "VAC")])
+def test_real_band_matches_oracle(gpu, tips, band, target):
+    name, molecule, mol_code, start, end = BANDS[band]
+    lines = read_lines(GOLD / name)
+    P, T, n = levels()
+    orc = O.Oracle(lines, tips, P, T, n, start, end, CUT, target=target, chi="none", mol_code=mol_code,
                    precision=O.FP64)
     _, ref, ev_ref = orc.run()
     lo_ref, hi_ref = orc.windows()
-    lo, hi = plan_windows(lines["nu"], START, END, CUT)      # 0-based; the oracle's are 1-based
+    lo, hi = plan_windows(lines["nu"], start, end, CUT)      # 0-based; the oracle's are 1-based
     assert np.array_equal(lo + 1, lo_ref) and np.array_equal(hi + 1, hi_ref)
-    run = dict(start_wv=START, end_wv=END, cutoff=CUT, target=target, molecule="CO", chi="none")
+    run = dict(start_wv=start, end_wv=end, cutoff=CUT, target=target, molecule=molecule, chi="none")
     with Context(lines, tips) as ctx:
         _, g64 = ctx.compute(Run(precision="fp64", **run), P, T, n, want64=True)
         g32 = ctx.compute(Run(precision="fp32c", **run), P, T, n)
@@ -57,7 +64,7 @@ def test_real_co_band_matches_oracle(gpu, tips, real, target):
     err, npts = rel_err(g64, ref, 0.0)
     assert npts == ref.size and err <= 1e-12, err
     e32, taint = check_fp32c(g32, ref, orc, tol=1e-5)
-    print(f"{target}: {int(ev_ref.sum())} evaluations, FP64 max err {err:.2e}, "
+    print(f"{band} {target}: {int(ev_ref.sum())} evaluations, FP64 max err {err:.2e}, "
           f"FP32c max err {e32:.2e} outside {taint} near-tie points")
     assert e32 <= 1e-5 and taint <= 1e-4 * ref.size
 
