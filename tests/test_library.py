@@ -63,3 +63,17 @@ def test_no_cpu_fallback_without_gpu(lib, tips):
     t = np.ascontiguousarray(tips)
     rc = lib.marfa_ctx_create(lines.ctypes.data, len(lines), t.ctypes.data, 74, 501, 0, ctypes.byref(h))
     assert rc == 110
+
+
+@pytest.mark.parametrize("name,start,end", [("co_hitran2020_1900_2400.lines", 2000.0, 2300.0),
+                                            ("o2_hitran2020_12900_13300.lines", 13000.0, 13200.0)])
+def test_plan_windows_on_reference_databases(lib, tips, name, start, end):
+    """Windows of the host planner on slices of the reference's own line
+    databases (tests/golden/make_real_golden.py) equal the oracle's."""
+    from marfa_b200.io import read_lines
+    lines = read_lines(ROOT / "tests" / "golden" / name)
+    lo, hi = plan_windows(lines["nu"], start, end, 25.0)
+    o = O.Oracle(lines, tips, [1.0], [296.0], [1e10], start, end, 25.0)
+    olo, ohi = o.windows()
+    assert np.array_equal(lo + 1, olo) and np.array_equal(hi + 1, ohi)
+

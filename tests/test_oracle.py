@@ -103,9 +103,13 @@ def test_mixed_and_fp64_maps_agree(cfg0, tips):
 
 
 def test_eval_counts_match_closed_form(cfg0, tips):
+    from pathlib import Path
+    from marfa_b200.io import read_lines
+    real = read_lines(Path(__file__).resolve().parent / "golden" / "co_hitran2020_1900_2400.lines")
     for lines, start, end, cut in ((cfg0.lines, 4000.0, 4100.0, 25.0),
                                    (edge_lines(), 4050.0, 4060.0, 25.0),
-                                   (edge_lines(), 4050.0, 4060.0, 0.75)):
+                                   (edge_lines(), 4050.0, 4060.0, 0.75),
+                                   (real, 2000.0, 2100.0, 25.0)):
         o = O.Oracle(lines, tips, [1.0], [296.0], [2.39e24], start, end, cut)
         _, _, ev = o.run(want64=False)
         lo, hi = o.windows()
